@@ -1,0 +1,221 @@
+"""TEST INFRASTRUCTURE ONLY: Python access to the checkers.
+
+* ``libchoracle.so``: the plain-C restatement of the reference's CH step
+  (ch_oracle.c), built by ``make -C oracle``.
+* ``_ref/libchref.so`` and ``_ref/chref_bench``: the reference CPU build
+  (the reference's own SfieldFD/Rand/PFApp sources plus the CHBasic model),
+  built by ``make -C oracle ref`` where the reference sources are present.
+* numpy restatements of the quantities the reference does not compute:
+  structure factor and its peak wavenumber, the linear-stability growth
+  factor, and the legacy-VTK text of ``SfieldFD::writeVTKFile``.
+
+Only tests, the smoke check and the benchmark's CPU-baseline leg import this
+module; the product never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_bin", "libchoracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libchref.so")
+REF_BENCH = os.path.join(HERE, "_ref", "chref_bench")
+REF_MESO = os.path.join(HERE, "_ref", "meso_ref")
+REFERENCE_SRC = "/root/reference"
+
+_i3 = ctypes.c_int * 3
+_d3 = ctypes.c_double * 3
+_d6 = ctypes.c_double * 6
+_dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+def build(reference: bool | None = None) -> None:
+    """Compile the C restatement, and the reference build when its sources exist."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if reference is None:
+        reference = os.path.isdir(os.path.join(REFERENCE_SRC, "src"))
+    if reference:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE_SRC}",
+                        f"-j{os.cpu_count() or 4}"], check=True)
+
+
+def _lib(path):
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built (make -C oracle [ref])")
+    return ctypes.CDLL(path)
+
+
+_oracle = None
+_ref = None
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        _oracle = _lib(ORACLE_SO)
+        L = _oracle
+        L.cho_ic.argtypes = [_i3, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_uint32, _dp]
+        L.cho_step.argtypes = [_i3, _d3, ctypes.c_double, ctypes.c_double, ctypes.c_double, _i3, _dp, _dp, _dp]
+        L.cho_run.argtypes = [_i3, _d3, ctypes.c_double, ctypes.c_double, ctypes.c_double, _i3, _dp, ctypes.c_int]
+        L.cho_run.restype = ctypes.c_int
+        L.cho_reduce.argtypes = [_i3, _d3, ctypes.c_double, _i3, _dp, _d6]
+        L.cho_reduce_f32.argtypes = [_i3, _d3, ctypes.c_double, _i3, _fp, _d6]
+        L.cho_rand_init.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+        L.cho_rand_u32.argtypes = [ctypes.c_void_p]
+        L.cho_rand_u32.restype = ctypes.c_uint32
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        _ref = _lib(REF_SO)
+        _ref.chref_run.argtypes = [_i3, _d3, ctypes.c_double, ctypes.c_double, ctypes.c_double, _i3, _dp,
+                                   ctypes.c_int, _dp]
+        _ref.chref_run.restype = ctypes.c_int
+        _ref.chref_ic.argtypes = [_i3, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_uint32, _dp]
+        _ref.chref_ic.restype = ctypes.c_int
+    return _ref
+
+
+def _as_field(c, dims):
+    nx, ny, nz = dims
+    a = np.ascontiguousarray(c, dtype=np.float64).reshape(nz, ny, nx)
+    return a
+
+
+def _ptr(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+# ----------------------------------------------------------------- restatement
+def mt_u32(seed: int, count: int) -> np.ndarray:
+    """First `count` outputs of the MT19937 restatement (rand.cpp:24-78)."""
+    L = oracle_lib()
+    state = ctypes.create_string_buffer(625 * 4)
+    L.cho_rand_init(state, seed)
+    return np.array([L.cho_rand_u32(state) for _ in range(count)], dtype=np.uint32)
+
+
+def ic(dims, co, amp, gaussian=False, seed=42) -> np.ndarray:
+    """Seeded initial condition, shape (nz, ny, nx), float64."""
+    nx, ny, nz = dims
+    out = np.empty((nz, ny, nx), dtype=np.float64)
+    oracle_lib().cho_ic(_i3(*dims), co, amp, int(bool(gaussian)), seed, _ptr(out))
+    return out
+
+
+def run(c, dims, spacing=(1.0, 1.0, 1.0), dt=0.01, M=1.0, kap=1.0, nsteps=1, bc=(1, 1, 1)) -> np.ndarray:
+    """nsteps CH steps of the C restatement; returns a new (nz, ny, nx) array."""
+    a = _as_field(c, dims).copy()
+    rc = oracle_lib().cho_run(_i3(*dims), _d3(*spacing), dt, M, kap, _i3(*bc), _ptr(a), nsteps)
+    if rc != 0:
+        raise MemoryError("oracle allocation failed")
+    return a
+
+
+def reduce(c, dims, spacing=(1.0, 1.0, 1.0), kap=1.0, bc=(1, 1, 1)) -> dict:
+    """Mass / energy diagnostics (ch_oracle.h), float64 or float32 input."""
+    nx, ny, nz = dims
+    out = _d6()
+    if np.asarray(c).dtype == np.float32:
+        a = np.ascontiguousarray(c, dtype=np.float32).reshape(nz, ny, nx)
+        oracle_lib().cho_reduce_f32(_i3(*dims), _d3(*spacing), kap, _i3(*bc), _ptr(a, _fp), out)
+    else:
+        a = _as_field(c, dims)
+        oracle_lib().cho_reduce(_i3(*dims), _d3(*spacing), kap, _i3(*bc), _ptr(a), out)
+    keys = ["mass", "mass_plain", "energy", "abs_mass", "max_abs", "nonfinite"]
+    return dict(zip(keys, list(out)))
+
+
+# ------------------------------------------------------------ reference build
+def ref_run(c, dims, spacing=(1.0, 1.0, 1.0), dt=0.01, M=1.0, kap=1.0, nsteps=1, bc=(1, 1, 1)) -> np.ndarray:
+    """nsteps steps of the reference CPU build (SfieldFD + CHBasic)."""
+    a = _as_field(c, dims)
+    out = np.empty_like(a)
+    ref_lib().chref_run(_i3(*dims), _d3(*spacing), dt, M, kap, _i3(*bc), _ptr(a), nsteps, _ptr(out))
+    return out
+
+
+def ref_ic(dims, co, amp, gaussian=False, seed=42) -> np.ndarray:
+    nx, ny, nz = dims
+    out = np.empty((nz, ny, nx), dtype=np.float64)
+    ref_lib().chref_ic(_i3(*dims), co, amp, int(bool(gaussian)), seed, _ptr(out))
+    return out
+
+
+# ------------------------------------------------- quantities with no reference
+def structure_factor(c, dims, spacing=(1.0, 1.0, 1.0), nbins=None):
+    """Radially binned S(k) = |FFT(c - <c>)|^2 / N and its first-moment
+    wavenumber k1 = sum(k S) / sum(S) over the binned spectrum.
+
+    Bin b holds |k| in [b*dk, (b+1)*dk) with dk = 2*pi/max(L); the k = 0
+    mode is excluded.  Returns (k_centres, S_binned, counts, k1)."""
+    nx, ny, nz = dims
+    a = np.asarray(c, dtype=np.float64).reshape(nz, ny, nx)
+    f = np.fft.fftn(a - a.mean())
+    s = (f.real ** 2 + f.imag ** 2) / a.size
+    kx = 2 * np.pi * np.fft.fftfreq(nx, d=spacing[0])
+    ky = 2 * np.pi * np.fft.fftfreq(ny, d=spacing[1])
+    kz = 2 * np.pi * np.fft.fftfreq(nz, d=spacing[2])
+    kk = np.sqrt(kz[:, None, None] ** 2 + ky[None, :, None] ** 2 + kx[None, None, :] ** 2)
+    dk = 2 * np.pi / max(nx * spacing[0], ny * spacing[1], nz * spacing[2])
+    if nbins is None:
+        nbins = int(np.floor(kk.max() / dk)) + 1
+    b = np.floor(kk / dk).astype(np.int64)
+    mask = (kk > 0) & (b < nbins)
+    sb = np.bincount(b[mask], weights=s[mask], minlength=nbins)
+    cnt = np.bincount(b[mask], minlength=nbins)
+    ksum = np.bincount(b[mask], weights=kk[mask], minlength=nbins)
+    kc = np.where(cnt > 0, ksum / np.maximum(cnt, 1), (np.arange(nbins) + 0.5) * dk)
+    sbar = np.where(cnt > 0, sb / np.maximum(cnt, 1), 0.0)
+    k1 = float((kc * sbar).sum() / sbar.sum()) if sbar.sum() > 0 else 0.0
+    return kc, sbar, cnt, k1
+
+
+def growth_factor(k_vec, dims_active, c0, kap, dt, M=1.0, spacing=(1.0, 1.0, 1.0)):
+    """Per-step amplification of a small Fourier mode about a uniform c0:
+    1 + dt*M*lam*(3*c0^2 - 1 - kap*lam), lam = -sum_d 4/dx_d^2 sin^2(k_d dx_d/2)."""
+    lam = 0.0
+    for kd, dd, on in zip(k_vec, spacing, dims_active):
+        if on:
+            lam -= 4.0 / dd ** 2 * np.sin(kd * dd / 2.0) ** 2
+    return 1.0 + dt * M * lam * (3 * c0 ** 2 - 1 - kap * lam)
+
+
+def vtk_text(c, dims, tag, iskip=1, jskip=1, kskip=1) -> str:
+    """Text of SfieldFD::writeVTKFile (SfieldFD.cpp:363-430) for one rank:
+    header, then one `%.3f` value per line, x fastest, with the skip rules
+    of :407-413 (x uses the global index test ig%iskip == 0 on 1-based ig;
+    y and z step by jskip/kskip from 1)."""
+    nx, ny, nz = dims
+    a = np.asarray(c, dtype=np.float64).reshape(nz, ny, nx)
+    d = "   "
+
+    def num(v):  # ostream default formatting of 1.0*skip
+        return f"{v:g}"
+
+    lines = ["# vtk DataFile Version 3.1", "VTK file containing grid data", "ASCII", " ",
+             "DATASET STRUCTURED_POINTS",
+             f"DIMENSIONS{d}{nx // iskip}{d}{ny // jskip}{d}{nz // kskip}",
+             f"ORIGIN {d}0{d}0{d}0",
+             f"SPACING{d}{num(1.0 * iskip)}{d}{num(1.0 * jskip)}{d}{num(1.0 * kskip)}",
+             " ",
+             f"POINT_DATA {(nx // iskip) * (ny // jskip) * (nz // kskip)}",
+             f"SCALARS {tag} float",
+             "LOOKUP_TABLE default"]
+    xs = [i for i in range(1, nx + 1) if i % iskip == 0]
+    for k in range(1, nz + 1, kskip):
+        for j in range(1, ny + 1, jskip):
+            row = a[k - 1, j - 1]
+            lines.extend(f"{row[i - 1]:.3f}" for i in xs)
+    return "\n".join(lines) + "\n"
