@@ -1,0 +1,216 @@
+/*
+ * mesogpu.h -- C ABI of libmesogpu.so, the B200 (sm_100a) Cahn-Hilliard
+ * phase-field step of mesoBasic's src/phase_field, re-designed for the GPU.
+ *
+ * Conventions
+ *   - Every int-returning call returns MG_OK (0) or a negative MG_E* code;
+ *     mg_last_error() gives a message for the calling thread.  No C++
+ *     exception crosses this boundary.
+ *   - Fields cross the boundary as dense host arrays of double, x fastest,
+ *     no ghost nodes: value of node (i,j,k) (0-based) at i + nx*(j + ny*k).
+ *     The reference's SfieldFD stores z fastest with one ghost layer
+ *     (SfieldFD.cpp:26-64); a caller holding such an array converts it.
+ *   - The library owns device memory; the caller owns host buffers.  Host
+ *     buffers in pinned memory (cudaHostAlloc) transfer fastest.
+ *   - A handle is driven by one host thread at a time.  Calls that enqueue
+ *     GPU work return before it finishes; mg_*_sync waits (with a limit).
+ *   - Two-dimensional runs are nz == 1, as in the reference (SfieldFD keeps
+ *     z ghosts equal to the single plane, SfieldFD.cpp:135-140).
+ */
+#ifndef MESOGPU_H
+#define MESOGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MG_OK 0
+#define MG_EINVAL (-1)      /* bad argument or unsupported configuration */
+#define MG_ENOMEM (-2)      /* device or host allocation failed / over budget */
+#define MG_ECUDA (-3)       /* a CUDA runtime or driver call failed */
+#define MG_ETIMEOUT (-4)    /* a bounded wait ran out */
+#define MG_ENONFINITE (-5)  /* the field holds NaN or Inf */
+#define MG_EDEVICE (-6)     /* a kernel reported an error (e.g. a bounded device wait ran out) */
+#define MG_ENOTFOUND (-7)   /* unknown job id */
+
+#define MG_FP64 0
+#define MG_FP32 1
+
+/* One simulation.  Keys of the reference input file in brackets. */
+typedef struct {
+    int nx, ny, nz;        /* grid [Domain/nx,ny,nz] */
+    double dx, dy, dz;     /* spacing [Domain/dx,dy,dz] */
+    double dt;             /* time step [Time/dt] */
+    double M;              /* constant mobility [PFApp/M] */
+    double kappa;          /* gradient coefficient [PFApp/kap] */
+    int bx, by, bz;        /* 1 periodic, 0 no-flux [PFApp/bx,by,bz] (SfieldFD.cpp:187-251) */
+    int precision;         /* MG_FP64: bit-identical to the reference build;
+                              MG_FP32: FP32 field, FP64 reductions */
+    int mass_correct;      /* MG_FP32 only: after each step the kernel sums the
+                              stored field in FP64; the next step adds the
+                              uniform correction (target - sum)/N before its
+                              FP32 rounding, so rounding errors of the field do
+                              not accumulate as a drift of total mass */
+} mg_ch_params;
+
+typedef struct {
+    double mass;       /* sum(c) dV, compensated FP64 */
+    double energy;     /* sum[(c^2-1)^2/4 + kappa/2 |grad+ c|^2] dV, compensated FP64 */
+    double abs_mass;   /* sum|c| dV */
+    double max_abs;    /* max |c| */
+    long long nonfinite; /* sites holding NaN/Inf */
+    long long step;    /* steps taken */
+} mg_ch_stats;
+
+/* Work decomposition of a job (see mg_autotune). */
+typedef struct {
+    int ty;      /* output rows per tile (3-D); 1 for 2-D jobs */
+    int nchunk;  /* z chunks (2-D: row chunks) */
+    int nbuf;    /* c planes in flight: 3 or 4 */
+    int path;    /* 0 tiled TMA kernel, 1 generic per-site kernel */
+} mg_tiling;
+
+typedef struct mg_ch mg_ch_t;
+typedef struct mg_batch mg_batch_t;
+typedef struct mg_server mg_server_t;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* mg_last_error(void);
+
+/* ----------------------------------------------------------------------
+ * Single simulation: the GPU body of a PFBaseClass model.
+ * -------------------------------------------------------------------- */
+
+/* Allocates the two field buffers of one simulation on `device`.
+ * Replaces: PFBaseClass::PFFactory + model constructor
+ * (PFBaseClass.cpp:26-55, TIPSphil.cpp:24-60, SfieldFD.cpp:26-64). */
+int mg_ch_create(const mg_ch_params* params, int device, mg_ch_t** out);
+
+/* Uploads a field (nx*ny*nz doubles; converted to FP32 for MG_FP32 jobs)
+ * and resets the step counter.  Replaces: the fill of c in
+ * initPhaseField (TIPSphil.cpp:86-96). */
+int mg_ch_set_field(mg_ch_t* h, const double* host);
+
+/* Enqueues nsteps explicit steps (one fused kernel launch each, replayed
+ * from a CUDA graph).  Replaces: nsteps calls of PFApp::stepForward ->
+ * updatePhaseField (PFApp.cpp:91-107, TIPSphil.cpp:113-211). */
+int mg_ch_step(mg_ch_t* h, int nsteps);
+
+/* Waits for the enqueued work, at most timeout_us microseconds (<0: no
+ * limit); reports kernel-side errors.  Replaces: MPI Barrier after a
+ * step (TIPSphil.cpp:129,192) as the completion point. */
+int mg_ch_sync(mg_ch_t* h, long long timeout_us);
+
+/* Downloads the current field (waits for enqueued work).  Replaces: the
+ * read of c in outputPhaseField -> SfieldFD::writeVTKFile (SfieldFD.cpp:363-430). */
+int mg_ch_get_field(mg_ch_t* h, double* host);
+
+/* Mass/energy diagnostics of the current field.  No reference counterpart
+ * (the reference logs neither).  Returns MG_ENONFINITE if any site is not
+ * finite (stats are still filled). */
+int mg_ch_reduce(mg_ch_t* h, mg_ch_stats* out);
+
+/* Radially binned structure factor S(k) = |FFT(c - <c>)|^2 / N of the
+ * current field (cuFFT + binning kernel), nbins bins of width
+ * dk = 2*pi/max(L); k[b] = mean |k| in bin b, S[b] = mean S in bin b;
+ * *k1 = sum(|k| S)/sum(S) over every mode in the bins (k = 0 excluded).  No reference counterpart (FFTW is linked by the
+ * reference but never executed, PFApp.cpp:46-48). */
+int mg_ch_structure_factor(mg_ch_t* h, int nbins, double* k, double* S, double* k1);
+
+/* The CUDA stream (cudaStream_t) the handle enqueues on, for event timing. */
+void* mg_ch_stream(mg_ch_t* h);
+
+/* Device pointer of the current field buffer (precision per params). */
+void* mg_ch_field_device(mg_ch_t* h);
+
+/* Steps taken (waits for enqueued work). */
+long long mg_ch_steps(mg_ch_t* h);
+
+int mg_ch_get_tiling(const mg_ch_t* h, mg_tiling* out);
+/* Overrides the decomposition; validates it against the kernel limits. */
+int mg_ch_set_tiling(mg_ch_t* h, const mg_tiling* t);
+
+/* Frees the device buffers.  Replaces: PFApp::~PFApp (PFApp.cpp:69-72). */
+void mg_ch_destroy(mg_ch_t* h);
+
+/* Times candidate decompositions of `params` on `device` (scratch fields,
+ * `trials` timed launches each) and returns the fastest.  Results are
+ * cached per (shape, precision) in the process and, when the environment
+ * variable MG_TUNE_CACHE names a file, in that JSON file, which
+ * mg_ch_create consults.  No reference counterpart. */
+int mg_autotune(const mg_ch_params* params, int device, int trials, mg_tiling* best, double* best_ms);
+
+/* ----------------------------------------------------------------------
+ * Host helpers over the reference's input surface.
+ * -------------------------------------------------------------------- */
+
+/* Seeded initial condition, reference loop order (x outer, then y, z):
+ * uniform: co + amp*(u - 0.5), u = MT19937 u32 / 4294967295;
+ * gaussian: co + amp*normal() (Box-Muller).  Replaces: the random fill of
+ * TIPSphil::initPhaseField (TIPSphil.cpp:86-96) with the reference's Rand
+ * (rand.cpp:24-94) seeded by `seed`. */
+int mg_ic_generate(const int dims[3], double co, double amp, int gaussian, unsigned seed, double* out);
+
+/* Appends one legacy-VTK block (header + `%.3f` values, x fastest, skip
+ * rules) to `path`, byte-identical to a single-rank
+ * SfieldFD::writeVTKFile(tag, step, iskip, jskip, kskip)
+ * (SfieldFD.cpp:363-430). */
+int mg_vtk_write(const char* path, const char* tag, const double* field, const int dims[3], int iskip, int jskip,
+                 int kskip);
+
+/* ----------------------------------------------------------------------
+ * Batch: many independent simulations of uneven sizes and parameters
+ * stepped by one persistent launch per precision class and step, replayed
+ * from a CUDA graph.  No reference counterpart (the reference runs one
+ * simulation per process).
+ * -------------------------------------------------------------------- */
+int mg_batch_create(const mg_ch_params* jobs, int njobs, int device, mg_batch_t** out);
+int mg_batch_set_field(mg_batch_t* b, int job, const double* host);
+int mg_batch_step(mg_batch_t* b, int nsteps);
+int mg_batch_sync(mg_batch_t* b, long long timeout_us);
+int mg_batch_get_field(mg_batch_t* b, int job, double* host);
+int mg_batch_reduce(mg_batch_t* b, int job, mg_ch_stats* out);
+void* mg_batch_stream(mg_batch_t* b);
+/* Items (tiles) and persistent CTAs of the batch's launches. */
+int mg_batch_info(const mg_batch_t* b, int* nitems, int* nctas, int* nlaunch_per_step);
+void mg_batch_destroy(mg_batch_t* b);
+
+/* ----------------------------------------------------------------------
+ * Server: continuous batching of simulation jobs under an HBM budget.
+ * A background thread admits queued jobs as memory and slots free up,
+ * steps all admitted jobs together (each to its own step count), and
+ * retires finished ones.  No reference counterpart.
+ * -------------------------------------------------------------------- */
+typedef struct {
+    long long submitted, completed, failed, running, queued;
+    double p50_ms, p99_ms;       /* completion latency, arrival -> result ready */
+    double mean_ms;
+    double sims_per_hour;        /* completed / wall time since the first arrival */
+    double site_updates_per_s;   /* sum(sites*steps) of completed jobs / wall time */
+    double hbm_in_use_gb, hbm_peak_gb;
+} mg_server_stats;
+
+#define MG_JOB_QUEUED 0
+#define MG_JOB_RUNNING 1
+#define MG_JOB_DONE 2
+#define MG_JOB_FAILED 3
+
+int mg_server_create(int device, double hbm_budget_gb, int max_jobs_in_flight, int steps_per_tick,
+                     mg_server_t** out);
+/* Copies `ic_host` (nx*ny*nz doubles) and queues the job; returns its id. */
+int mg_server_submit(mg_server_t* s, const mg_ch_params* params, const double* ic_host, long long nsteps,
+                     long long* job_id);
+int mg_server_poll(mg_server_t* s, long long job_id, int* state);
+/* Waits (bounded) for the job, then copies its final field (may be NULL)
+ * and stats and releases it. */
+int mg_server_result(mg_server_t* s, long long job_id, long long timeout_us, double* field_out,
+                     mg_ch_stats* stats);
+int mg_server_stats_get(mg_server_t* s, mg_server_stats* out);
+/* Stops accepting jobs, finishes the admitted ones, joins the thread. */
+void mg_server_destroy(mg_server_t* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MESOGPU_H */

@@ -1,0 +1,297 @@
+// C ABI of libmesogpu.so (declared in include/mesogpu.h): single
+// simulations, batches and the autotuner.  The server lives in server.cu,
+// host I/O (initial condition, VTK) in host_io.cpp.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstdlib>
+#include <memory>
+#include <new>
+#include <vector>
+
+#include "engine.h"
+
+struct mg_ch {
+    mg::Engine eng;
+    mg::Job* job = nullptr;
+};
+
+struct mg_batch {
+    mg::Engine eng;
+    std::vector<mg::Job*> jobs;
+};
+
+using mg::fail;
+
+extern "C" {
+
+const char* mg_last_error(void) { return mg::last_error(); }
+
+int mg_ch_create(const mg_ch_params* params, int device, mg_ch_t** out)
+{
+    mg::clear_error();
+    if (!params || !out) return fail(MG_EINVAL, "null argument");
+    *out = nullptr;
+    mg::Geometry g;
+    MG_TRY(mg::make_geometry(*params, &g));  // argument errors before any device work
+    std::unique_ptr<mg_ch> h(new (std::nothrow) mg_ch);
+    if (!h) return fail(MG_ENOMEM, "host allocation failed");
+    MG_TRY(h->eng.init(device, 1));
+    MG_TRY(h->eng.add_job(*params, -1, &h->job));
+    *out = h.release();
+    return MG_OK;
+}
+
+int mg_ch_set_field(mg_ch_t* h, const double* host)
+{
+    mg::clear_error();
+    if (!h) return fail(MG_EINVAL, "null handle");
+    return h->eng.upload(h->job, host, -1);
+}
+
+int mg_ch_step(mg_ch_t* h, int nsteps)
+{
+    mg::clear_error();
+    if (!h) return fail(MG_EINVAL, "null handle");
+    return h->eng.enqueue_steps(nsteps);
+}
+
+int mg_ch_sync(mg_ch_t* h, long long timeout_us)
+{
+    mg::clear_error();
+    if (!h) return fail(MG_EINVAL, "null handle");
+    return h->eng.sync(timeout_us);
+}
+
+int mg_ch_get_field(mg_ch_t* h, double* host)
+{
+    mg::clear_error();
+    if (!h) return fail(MG_EINVAL, "null handle");
+    return h->eng.download(h->job, host);
+}
+
+int mg_ch_reduce(mg_ch_t* h, mg_ch_stats* out)
+{
+    mg::clear_error();
+    if (!h) return fail(MG_EINVAL, "null handle");
+    return h->eng.diagnostics(h->job, out);
+}
+
+int mg_ch_structure_factor(mg_ch_t* h, int nbins, double* k, double* S, double* k1)
+{
+    mg::clear_error();
+    if (!h) return fail(MG_EINVAL, "null handle");
+    return h->eng.structure_factor(h->job, nbins, k, S, k1);
+}
+
+void* mg_ch_stream(mg_ch_t* h) { return h ? (void*)h->eng.stream : nullptr; }
+
+void* mg_ch_field_device(mg_ch_t* h)
+{
+    if (!h) return nullptr;
+    mg::JobDev st;
+    if (h->eng.read_state(h->job, &st) != MG_OK) return nullptr;
+    return h->job->buf[st.step & 1];
+}
+
+long long mg_ch_steps(mg_ch_t* h)
+{
+    if (!h) return -1;
+    mg::JobDev st;
+    if (h->eng.read_state(h->job, &st) != MG_OK) return -1;
+    return st.step;
+}
+
+int mg_ch_get_tiling(const mg_ch_t* h, mg_tiling* out)
+{
+    mg::clear_error();
+    if (!h || !out) return fail(MG_EINVAL, "null argument");
+    *out = h->job->tiling;
+    return MG_OK;
+}
+
+int mg_ch_set_tiling(mg_ch_t* h, const mg_tiling* t)
+{
+    mg::clear_error();
+    if (!h || !t) return fail(MG_EINVAL, "null argument");
+    return h->eng.set_tiling(h->job, *t);
+}
+
+void mg_ch_destroy(mg_ch_t* h) { delete h; }
+
+// ------------------------------------------------------------- autotune
+static int time_tiling(mg_ch* h, const mg_tiling& t, int trials, double* ms)
+{
+    MG_TRY(h->eng.set_tiling(h->job, t));
+    MG_TRY(h->eng.enqueue_steps(2));  // warm-up (also captures the graph)
+    cudaEvent_t e0, e1;
+    MG_CUDA(cudaEventCreate(&e0));
+    MG_CUDA(cudaEventCreate(&e1));
+    cudaEventRecord(e0, h->eng.stream);
+    int rc = h->eng.enqueue_steps(trials);
+    cudaEventRecord(e1, h->eng.stream);
+    cudaEventSynchronize(e1);
+    float f = 0.f;
+    cudaEventElapsedTime(&f, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    MG_TRY(rc);
+    MG_TRY(h->eng.sync(-1));
+    *ms = f / trials;
+    return MG_OK;
+}
+
+int mg_autotune(const mg_ch_params* params, int device, int trials, mg_tiling* best, double* best_ms)
+{
+    mg::clear_error();
+    if (!params || !best) return fail(MG_EINVAL, "null argument");
+    if (trials < 1) trials = 10;
+    mg_ch_t* h = nullptr;
+    MG_TRY(mg_ch_create(params, device, &h));
+    std::unique_ptr<mg_ch> guard(h);
+    const mg::Geometry& g = h->job->g;
+    if (!mg::tma_shape_ok(g)) {
+        *best = mg_tiling{1, 1, 4, 1};
+        if (best_ms) *best_ms = -1.0;
+        return MG_OK;
+    }
+    MG_CUDA(cudaMemsetAsync(h->job->buf[0], 0, g.n * g.es, h->eng.stream));
+    MG_CUDA(cudaMemsetAsync(h->job->buf[1], 0, g.n * g.es, h->eng.stream));
+    std::vector<mg_tiling> cands;
+    std::vector<int> tys;
+    if (g.flat) tys.push_back(1);
+    else
+        for (int ty = 2; ty <= std::min(g.lny, 40); ty += 2) tys.push_back(ty);
+    for (int nbuf = 3; nbuf <= 4; ++nbuf)
+        for (int ty : tys) {
+            mg_tiling t{ty, 1, nbuf, 0};
+            mg::TilePlan pl;
+            if (mg::plan_tiling(g, t, h->eng.info, &pl) != MG_OK) {
+                mg::clear_error();
+                continue;
+            }
+            int occ = 1;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mg::step_kernel(g.es == 4, g.flat, nbuf),
+                                                              pl.block, pl.smem) != cudaSuccess)
+                continue;
+            occ = std::max(occ, 1);
+            const int slots = h->eng.info.sms * occ;
+            std::vector<int> ncs;
+            for (int mult = 1; mult <= 3; ++mult) {
+                int nc = std::max(1, mult * slots / pl.ntile);
+                ncs.push_back(nc);
+                if (nc > 1) ncs.push_back(nc & ~1);
+            }
+            std::sort(ncs.begin(), ncs.end());
+            ncs.erase(std::unique(ncs.begin(), ncs.end()), ncs.end());
+            for (int nc : ncs) {
+                if (nc > g.lnz / 4 && nc > 1) continue;
+                t.nchunk = nc;
+                cands.push_back(t);
+            }
+        }
+    double bms = 1e30;
+    mg_tiling bt = h->job->tiling;
+    for (const mg_tiling& t : cands) {
+        double ms;
+        if (time_tiling(h, t, trials, &ms) != MG_OK) {
+            mg::clear_error();
+            continue;
+        }
+        if (ms < bms) {
+            bms = ms;
+            bt = t;
+        }
+    }
+    if (bms >= 1e30) return fail(MG_ECUDA, "autotune: no candidate ran");
+    mg::tune_store(mg::tune_key(g), bt, bms);
+    *best = bt;
+    if (best_ms) *best_ms = bms;
+    return MG_OK;
+}
+
+// ---------------------------------------------------------------- batch
+int mg_batch_create(const mg_ch_params* jobs, int njobs, int device, mg_batch_t** out)
+{
+    mg::clear_error();
+    if (!jobs || njobs < 1 || !out) return fail(MG_EINVAL, "bad arguments");
+    *out = nullptr;
+    for (int i = 0; i < njobs; ++i) {
+        mg::Geometry g;
+        if (mg::make_geometry(jobs[i], &g) != MG_OK) return fail(MG_EINVAL, "job %d: %s", i, mg::last_error());
+    }
+    std::unique_ptr<mg_batch> b(new (std::nothrow) mg_batch);
+    if (!b) return fail(MG_ENOMEM, "host allocation failed");
+    MG_TRY(b->eng.init(device, njobs));
+    for (int i = 0; i < njobs; ++i) {
+        mg::Job* j = nullptr;
+        int rc = b->eng.add_job(jobs[i], -1, &j);
+        if (rc != MG_OK) return fail(rc, "job %d: %s", i, mg::last_error());
+        b->jobs.push_back(j);
+    }
+    *out = b.release();
+    return MG_OK;
+}
+
+static int batch_job(mg_batch_t* b, int job, mg::Job** j)
+{
+    if (!b) return fail(MG_EINVAL, "null handle");
+    if (job < 0 || job >= (int)b->jobs.size()) return fail(MG_EINVAL, "job %d out of range", job);
+    *j = b->jobs[job];
+    return MG_OK;
+}
+
+int mg_batch_set_field(mg_batch_t* b, int job, const double* host)
+{
+    mg::clear_error();
+    mg::Job* j;
+    MG_TRY(batch_job(b, job, &j));
+    return b->eng.upload(j, host, -1);
+}
+
+int mg_batch_step(mg_batch_t* b, int nsteps)
+{
+    mg::clear_error();
+    if (!b) return fail(MG_EINVAL, "null handle");
+    return b->eng.enqueue_steps(nsteps);
+}
+
+int mg_batch_sync(mg_batch_t* b, long long timeout_us)
+{
+    mg::clear_error();
+    if (!b) return fail(MG_EINVAL, "null handle");
+    return b->eng.sync(timeout_us);
+}
+
+int mg_batch_get_field(mg_batch_t* b, int job, double* host)
+{
+    mg::clear_error();
+    mg::Job* j;
+    MG_TRY(batch_job(b, job, &j));
+    return b->eng.download(j, host);
+}
+
+int mg_batch_reduce(mg_batch_t* b, int job, mg_ch_stats* out)
+{
+    mg::clear_error();
+    mg::Job* j;
+    MG_TRY(batch_job(b, job, &j));
+    return b->eng.diagnostics(j, out);
+}
+
+void* mg_batch_stream(mg_batch_t* b) { return b ? (void*)b->eng.stream : nullptr; }
+
+int mg_batch_info(const mg_batch_t* b, int* nitems, int* nctas, int* nlaunch)
+{
+    mg::clear_error();
+    if (!b) return fail(MG_EINVAL, "null handle");
+    if (nitems) *nitems = b->eng.nitems_total();
+    if (nctas) *nctas = b->eng.nctas_total();
+    if (nlaunch) *nlaunch = b->eng.nlaunch_per_step();
+    return MG_OK;
+}
+
+void mg_batch_destroy(mg_batch_t* b) { delete b; }
+
+}  // extern "C"

@@ -1,0 +1,81 @@
+// Types shared by the step kernels and the host engine.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mg {
+
+enum JobFlags : int {
+    JF_PER_X = 1 << 0,
+    JF_PER_Y = 1 << 1,
+    JF_PER_Z = 1 << 2,
+    JF_DIV_X = 1 << 3,  // divide by dx^2 (dx^2 not a power of two), FP64 only
+    JF_DIV_Y = 1 << 4,
+    JF_DIV_Z = 1 << 5,
+    JF_MASS = 1 << 6,  // FP32 mass-defect feedback
+    JF_FLAT = 1 << 7,  // logical ny == 1
+};
+
+enum DeviceError : int {
+    DEV_OK = 0,
+    DEV_TMA_TIMEOUT = 1,  // a TMA completion wait ran out of polls
+};
+
+// Per-job state in device memory.  The host fills the parameters; `delta`,
+// `mass_last`, `step`, `done` and `err` are updated by the kernels.
+struct alignas(16) JobDev {
+    void* buf[2];               // ping-pong fields; step s reads buf[s & 1]
+    const CUtensorMap* tmap;    // [2 buffers][body map (bw x ty x 1), row map (bw x 1 x 1)]
+    double2* partial;           // per-item mass pairs (JF_MASS)
+    int nx, ny, nz;             // logical dims (2-D jobs: nx, 1, ny)
+    int ty;                     // output rows per tile (1 when flat)
+    int ntile, nchunk;          // y tiles x z chunks = items
+    int flags;                  // JobFlags
+    int bw;                     // TMA box width = shared-memory piece width
+    double cx, cy, cz;          // 1/d^2 (multiply) or d^2 (divide when JF_DIV_*)
+    double kap, dtM;            // kappa, dt*M
+    double inv_nsites;          // 1 / (nx*ny*nz)
+    double mass_target;         // sum(c) of the uploaded field (JF_MASS)
+    double delta;               // uniform correction for the next step (JF_MASS)
+    double mass_last;           // sum(c) after the last step (JF_MASS)
+    long long step;             // steps taken
+    long long target;           // the job stops stepping here
+    unsigned int done;          // items finished in the running launch
+    int err;                    // DeviceError
+};
+
+struct StepArgs {
+    JobDev* jobs;           // all job slots of the engine
+    const int* job_slot;    // [njobs] slot of the launch's job j
+    const int* item_begin;  // [njobs + 1], items of job j: [item_begin[j], item_begin[j+1])
+    int njobs;
+    int nitems;
+    int cplane;             // shared-memory elements per c plane (max over jobs)
+    int mplane;             // shared-memory elements per mu plane (max over jobs)
+    long long spin_limit;   // polls before a TMA wait gives up
+    int* err;               // launch-wide error word (max of DeviceError)
+    uint32_t tx_extra;      // test hook: bytes expected beyond a plane (0 in use);
+                            // nonzero makes every TMA wait run out
+};
+
+// Shared-memory header: NBUF mbarriers, broadcast words, reduction scratch.
+struct SmemHead {
+    uint64_t bar[8];
+    long long step;
+    int flag;
+    int abort;
+    double delta;
+    double2 red[32];
+};
+
+// Diagnostics of the current field of one job (see ch_diag_partial).
+struct Diag {
+    double mass, energy, abs_mass, max_abs, nonfinite;
+};
+
+constexpr int kDiagBlocks = 592;   // 4 x 148 SMs
+constexpr int kDiagThreads = 256;
+
+}  // namespace mg

@@ -1,0 +1,976 @@
+// Host engine of libmesogpu: job setup, tensor maps, launch groups, CUDA
+// graphs, transfers, diagnostics.  See engine.h.
+#include "engine.h"
+#include "ch_kernels.cuh"
+
+#include <cufft.h>
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <thread>
+
+namespace mg {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string t_err;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_err = buf;
+    return code;
+}
+void clear_error() { t_err.clear(); }
+const char* last_error() { return t_err.c_str(); }
+
+// ------------------------------------------------------------ device info
+int device_info(int device, DevInfo* out)
+{
+    static std::mutex mu;
+    static std::map<int, DevInfo> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(device);
+    if (it != cache.end()) {
+        *out = it->second;
+        return MG_OK;
+    }
+    int count = 0;
+    MG_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) return fail(MG_EINVAL, "device %d not present (%d devices)", device, count);
+    cudaDeviceProp prop;
+    MG_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) return fail(MG_EINVAL, "device %d is sm_%d%d; this library is built for sm_100a", device,
+                                     prop.major, prop.minor);
+    DevInfo d;
+    d.sms = prop.multiProcessorCount;
+    d.smem_optin = prop.sharedMemPerBlockOptin;
+    d.total_mem = prop.totalGlobalMem;
+    d.major = prop.major;
+    d.minor = prop.minor;
+    cache[device] = d;
+    *out = d;
+    return MG_OK;
+}
+
+// ------------------------------------------------------------ tensor maps
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static int get_encode(EncodeTiledFn* fn)
+{
+    static EncodeTiledFn cached = nullptr;
+    static std::once_flag once;
+    static cudaError_t status = cudaSuccess;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        status = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+        if (status == cudaSuccess && q == cudaDriverEntryPointSuccess) cached = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    if (!cached) return fail(MG_ECUDA, "cuTensorMapEncodeTiled unavailable (%s)", cudaGetErrorString(status));
+    *fn = cached;
+    return MG_OK;
+}
+
+// body map: box (bw, ty, 1); row map: box (bw, 1, 1)
+static int encode_maps(const Job& j, CUtensorMap host_maps[4])
+{
+    EncodeTiledFn enc;
+    MG_TRY(get_encode(&enc));
+    const Geometry& g = j.g;
+    const int bw = std::min(g.lnx, 256);
+    for (int b = 0; b < 2; ++b) {
+        cuuint64_t dims[3] = {(cuuint64_t)g.lnx, (cuuint64_t)g.lny, (cuuint64_t)g.lnz};
+        cuuint64_t strides[2] = {(cuuint64_t)g.lnx * g.es, (cuuint64_t)g.lnx * g.lny * g.es};
+        cuuint32_t estr[3] = {1, 1, 1};
+        const CUtensorMapDataType dt = g.es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+        for (int m = 0; m < 2; ++m) {
+            cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)(m == 0 ? (g.flat ? 1 : j.tiling.ty) : 1), 1};
+            CUresult r = enc(&host_maps[2 * b + m], dt, 3, j.buf[b], dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return fail(MG_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+        }
+    }
+    return MG_OK;
+}
+
+// ------------------------------------------------------------ geometry
+int validate_params(const mg_ch_params& p)
+{
+    if (p.nx < 1 || p.ny < 1 || p.nz < 1) return fail(MG_EINVAL, "grid %dx%dx%d: every dimension must be >= 1", p.nx, p.ny, p.nz);
+    const double n = (double)p.nx * p.ny * p.nz;
+    if (n > 4.0e10) return fail(MG_EINVAL, "grid of %.3g sites is too large", n);
+    if (!(p.dx > 0) || !(p.dy > 0) || !(p.dz > 0) || !std::isfinite(p.dx) || !std::isfinite(p.dy) || !std::isfinite(p.dz))
+        return fail(MG_EINVAL, "grid spacing must be positive and finite");
+    if (!std::isfinite(p.dt) || !std::isfinite(p.M) || !std::isfinite(p.kappa))
+        return fail(MG_EINVAL, "dt, M and kappa must be finite");
+    if ((p.bx != 0 && p.bx != 1) || (p.by != 0 && p.by != 1) || (p.bz != 0 && p.bz != 1))
+        return fail(MG_EINVAL, "bx, by, bz must be 0 (no-flux) or 1 (periodic)");
+    if (p.precision != MG_FP64 && p.precision != MG_FP32) return fail(MG_EINVAL, "precision must be MG_FP64 or MG_FP32");
+    if (p.mass_correct && p.precision != MG_FP32) return fail(MG_EINVAL, "mass_correct applies to MG_FP32 only");
+    return MG_OK;
+}
+
+int make_geometry(const mg_ch_params& p, Geometry* out)
+{
+    MG_TRY(validate_params(p));
+    Geometry g;
+    g.es = p.precision == MG_FP32 ? 4 : 8;
+    if (p.nz == 1 && p.ny > 1) {
+        // 2-D: run as (nx, 1, ny); the reference's z Laplacian term is 0
+        g.lnx = p.nx, g.lny = 1, g.lnz = p.ny;
+        g.lsx = p.dx, g.lsy = p.dz, g.lsz = p.dy;
+        g.perx = p.bx, g.pery = 1, g.perz = p.by;
+        g.flat = true;
+    } else {
+        g.lnx = p.nx, g.lny = p.ny, g.lnz = p.nz;
+        g.lsx = p.dx, g.lsy = p.dy, g.lsz = p.dz;
+        g.perx = p.bx, g.pery = p.by, g.perz = p.bz;
+        g.flat = (p.ny == 1);
+    }
+    g.n = (size_t)p.nx * p.ny * p.nz;
+    *out = g;
+    return MG_OK;
+}
+
+bool tma_shape_ok(const Geometry& g)
+{
+    const int vec = 16 / g.es;
+    if (g.lnx % vec != 0) return false;
+    if (g.lnx > 256 && g.lnx % 256 != 0) return false;
+    const int bw = std::min(g.lnx, 256);
+    if ((bw * g.es) % 128 != 0) return false;  // 128-byte aligned TMA destinations
+    if (g.flat && g.lnx / vec > 512) return false;
+    if (!g.flat && g.lny < 2) return false;
+    return true;
+}
+
+static int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+int plan_tiling(const Geometry& g, const mg_tiling& t, const DevInfo& d, TilePlan* out)
+{
+    TilePlan pl;
+    if (t.path == 1) {
+        pl.tma_ok = false;
+        pl.block = 256;
+        pl.nitems = 1;
+        *out = pl;
+        return MG_OK;
+    }
+    if (t.path != 0) return fail(MG_EINVAL, "tiling path must be 0 or 1");
+    if (!tma_shape_ok(g)) return fail(MG_EINVAL, "shape %dx%dx%d (%s) is not taken by the tiled kernel", g.lnx, g.lny,
+                                      g.lnz, g.es == 4 ? "fp32" : "fp64");
+    if (t.nbuf != 3 && t.nbuf != 4) return fail(MG_EINVAL, "nbuf must be 3 or 4");
+    if (t.nchunk < 1 || t.nchunk > g.lnz) return fail(MG_EINVAL, "nchunk %d outside [1, %d]", t.nchunk, g.lnz);
+    const int vec = 16 / g.es;
+    const int nq = g.lnx / vec;
+    int CY, MY, ntr;
+    if (g.flat) {
+        if (t.ty != 1) return fail(MG_EINVAL, "2-D jobs use ty = 1");
+        CY = MY = 1;
+        ntr = 1;
+        pl.ntile = 1;
+    } else {
+        if (t.ty < 2 || t.ty % 2 != 0 || t.ty > g.lny || t.ty > 254)
+            return fail(MG_EINVAL, "ty %d must be even, >= 2 and <= ny (%d)", t.ty, g.lny);
+        CY = t.ty + 4;
+        MY = t.ty + 2;
+        ntr = MY / 2;
+        pl.ntile = (g.lny + t.ty - 1) / t.ty;
+    }
+    pl.block = round_up(nq * ntr, 32);
+    if (pl.block > 512) return fail(MG_EINVAL, "tile needs %d threads (> 512); lower ty", nq * ntr);
+    pl.cplane = round_up(CY * g.lnx, 32);
+    pl.mplane = round_up(MY * g.lnx, 32);
+    const size_t head = (sizeof(SmemHead) + 127) / 128 * 128 + 128;  // + alignment slack
+    pl.smem = head + (size_t)t.nbuf * pl.cplane * g.es + (size_t)3 * pl.mplane * g.es;
+    if (pl.smem > d.smem_optin)
+        return fail(MG_EINVAL, "tile needs %zu bytes of shared memory (> %zu); lower ty", pl.smem, d.smem_optin);
+    pl.nitems = pl.ntile * t.nchunk;
+    pl.tma_ok = true;
+    *out = pl;
+    return MG_OK;
+}
+
+StepKernel step_kernel(bool fp32, bool flat, int nbuf)
+{
+    if (fp32) {
+        if (flat) return nbuf == 3 ? ch_step_kernel<float, 3, true> : ch_step_kernel<float, 4, true>;
+        return nbuf == 3 ? ch_step_kernel<float, 3, false> : ch_step_kernel<float, 4, false>;
+    }
+    if (flat) return nbuf == 3 ? ch_step_kernel<double, 3, true> : ch_step_kernel<double, 4, true>;
+    return nbuf == 3 ? ch_step_kernel<double, 3, false> : ch_step_kernel<double, 4, false>;
+}
+
+int prepare_kernels(const DevInfo& d)
+{
+    for (int f32 = 0; f32 < 2; ++f32)
+        for (int fl = 0; fl < 2; ++fl)
+            for (int nb = 3; nb <= 4; ++nb)
+                MG_CUDA(cudaFuncSetAttribute(step_kernel(f32, fl, nb), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)d.smem_optin));
+    return MG_OK;
+}
+
+static int occupancy(const Geometry& g, const mg_tiling& t, const TilePlan& pl, int* occ)
+{
+    MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, step_kernel(g.es == 4, g.flat, t.nbuf), pl.block,
+                                                          pl.smem));
+    if (*occ < 1) *occ = 1;
+    return MG_OK;
+}
+
+mg_tiling default_tiling(const Geometry& g, const DevInfo& d, int device)
+{
+    (void)device;
+    mg_tiling best{1, 1, 4, 1};
+    if (!tma_shape_ok(g)) return best;
+    std::string key = tune_key(g);
+    mg_tiling tuned;
+    if (tune_lookup(key, &tuned)) {
+        TilePlan pl;
+        if (plan_tiling(g, tuned, d, &pl) == MG_OK) return tuned;
+        clear_error();
+    }
+    // heuristic: the deepest tile (fewest halo rows) that keeps two CTAs per
+    // SM, then enough z chunks to fill every CTA slot once, even count so
+    // neighbouring chunks march towards / away from each other
+    double best_score = -1.0;
+    for (int nbuf = 4; nbuf >= 3; --nbuf) {
+        std::vector<int> tys;
+        if (g.flat) tys.push_back(1);
+        else
+            for (int ty = 2; ty <= std::min(g.lny, 32); ty += 2) tys.push_back(ty);
+        for (int ty : tys) {
+            mg_tiling t{ty, 1, nbuf, 0};
+            TilePlan pl;
+            if (plan_tiling(g, t, d, &pl) != MG_OK) {
+                clear_error();
+                continue;
+            }
+            int occ = 1;
+            if (occupancy(g, t, pl, &occ) != MG_OK) {
+                clear_error();
+                continue;
+            }
+            const int slots = d.sms * occ;
+            int nchunk = std::max(1, slots / pl.ntile);
+            const int minplanes = g.flat ? 8 : 16;
+            nchunk = std::min(nchunk, std::max(1, g.lnz / minplanes));
+            if (nchunk > 1 && (nchunk & 1)) nchunk -= 1;
+            const int items = pl.ntile * nchunk;
+            // efficiency: filled slots x halo overheads
+            const double fill = std::min(1.0, (double)items / slots);
+            const double rows = g.flat ? 1.0 : (double)ty / (ty + 4);
+            const double planes = (double)(g.lnz / nchunk) / (g.lnz / nchunk + 4);
+            const double occw = occ >= 2 ? 1.0 : 0.85;
+            const double score = fill * std::sqrt(rows) * planes * occw * (nbuf == 4 ? 1.0 : 0.97);
+            if (score > best_score) {
+                best_score = score;
+                best = mg_tiling{ty, nchunk, nbuf, 0};
+            }
+        }
+    }
+    return best;
+}
+
+// ------------------------------------------------------------ autotune cache
+static std::mutex g_tune_mu;
+static std::map<std::string, std::pair<mg_tiling, double>> g_tune;
+static bool g_tune_loaded = false;
+
+std::string tune_key(const Geometry& g)
+{
+    char buf[128];
+    std::snprintf(buf, sizeof buf, "%s:%dx%dx%d:%s", g.es == 4 ? "fp32" : "fp64", g.lnx, g.lny, g.lnz,
+                  g.flat ? "flat" : "3d");
+    return buf;
+}
+
+static void tune_load_file()
+{
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* path = std::getenv("MG_TUNE_CACHE");
+    if (!path) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    std::string s;
+    char buf[4096];
+    size_t k;
+    while ((k = std::fread(buf, 1, sizeof buf, f)) > 0) s.append(buf, k);
+    std::fclose(f);
+    // entries: "key": [ty, nchunk, nbuf, path, ms]
+    size_t pos = 0;
+    while ((pos = s.find('"', pos)) != std::string::npos) {
+        size_t end = s.find('"', pos + 1);
+        if (end == std::string::npos) break;
+        std::string key = s.substr(pos + 1, end - pos - 1);
+        size_t lb = s.find('[', end);
+        if (lb == std::string::npos) break;
+        mg_tiling t;
+        double ms = 0;
+        if (std::sscanf(s.c_str() + lb, "[%d, %d, %d, %d, %lf]", &t.ty, &t.nchunk, &t.nbuf, &t.path, &ms) == 5)
+            g_tune[key] = {t, ms};
+        pos = s.find(']', lb);
+        if (pos == std::string::npos) break;
+    }
+}
+
+bool tune_lookup(const std::string& key, mg_tiling* t)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    tune_load_file();
+    auto it = g_tune.find(key);
+    if (it == g_tune.end()) return false;
+    *t = it->second.first;
+    return true;
+}
+
+void tune_store(const std::string& key, const mg_tiling& t, double ms)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    tune_load_file();
+    g_tune[key] = {t, ms};
+    const char* path = std::getenv("MG_TUNE_CACHE");
+    if (!path) return;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return;
+    std::fprintf(f, "{\n");
+    size_t i = 0;
+    for (auto& kv : g_tune) {
+        std::fprintf(f, "  \"%s\": [%d, %d, %d, %d, %.6f]%s\n", kv.first.c_str(), kv.second.first.ty,
+                     kv.second.first.nchunk, kv.second.first.nbuf, kv.second.first.path, kv.second.second,
+                     ++i < g_tune.size() ? "," : "");
+    }
+    std::fprintf(f, "}\n");
+    std::fclose(f);
+}
+
+// ------------------------------------------------------------------ Job
+size_t Job::device_bytes() const
+{
+    return 2 * g.n * g.es + 4 * sizeof(CUtensorMap) + (size_t)std::max(plan.nitems, 1) * sizeof(double2);
+}
+
+static void fill_jobdev(const Job& j, JobDev* jd)
+{
+    std::memset(jd, 0, sizeof *jd);
+    const Geometry& g = j.g;
+    jd->buf[0] = j.buf[0];
+    jd->buf[1] = j.buf[1];
+    jd->tmap = j.d_tmap;
+    jd->partial = j.d_partial;
+    jd->nx = g.lnx;
+    jd->ny = g.lny;
+    jd->nz = g.lnz;
+    jd->ty = j.tiling.ty;
+    jd->ntile = std::max(j.plan.ntile, 1);
+    jd->nchunk = j.tiling.nchunk;
+    jd->bw = std::min(g.lnx, 256);
+    int flags = 0;
+    if (g.perx) flags |= JF_PER_X;
+    if (g.pery) flags |= JF_PER_Y;
+    if (g.perz) flags |= JF_PER_Z;
+    if (g.flat) flags |= JF_FLAT;
+    if (j.p.mass_correct && g.es == 4) flags |= JF_MASS;
+    const double sp[3] = {g.lsx, g.lsy, g.lsz};
+    double coef[3];
+    for (int a = 0; a < 3; ++a) {
+        const double d2 = sp[a] * sp[a];
+        int e;
+        const bool pow2 = std::frexp(d2, &e) == 0.5;
+        if (g.es == 8 && !pow2) {
+            coef[a] = d2;  // divide, as the reference does
+            flags |= (JF_DIV_X << a);
+        } else {
+            coef[a] = 1.0 / d2;  // exact for powers of two
+        }
+    }
+    jd->cx = coef[0];
+    jd->cy = coef[1];
+    jd->cz = coef[2];
+    jd->flags = flags;
+    jd->kap = j.p.kappa;
+    jd->dtM = j.p.dt * j.p.M;
+    jd->inv_nsites = 1.0 / (double)g.n;
+    jd->target = j.target < 0 ? LLONG_MAX : j.target;
+}
+
+// ------------------------------------------------------------------ Engine
+Engine::~Engine()
+{
+    if (stream) cudaStreamSynchronize(stream);
+    for (Job* j : jobs) {
+        cudaFree(j->buf[0]);
+        cudaFree(j->buf[1]);
+        cudaFree(j->d_tmap);
+        cudaFree(j->d_partial);
+        delete j;
+    }
+    jobs.clear();
+    drop_graphs();
+    free_groups();
+    cudaFree(d_jobs_);
+    cudaFree(d_err_);
+    cudaFree(d_stage_);
+    cudaFree(d_diag_part_);
+    cudaFree(d_diag_max_);
+    cudaFree(d_diag_bad_);
+    cudaFree(d_diag_);
+    cudaFreeHost(h_diag_);
+    cudaFreeHost(h_state_);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+int Engine::init(int dev, int capacity)
+{
+    device = dev;
+    MG_TRY(device_info(dev, &info));
+    MG_CUDA(cudaSetDevice(dev));
+    MG_TRY(prepare_kernels(info));
+    MG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    capacity_ = capacity;
+    MG_CUDA(cudaMalloc(&d_jobs_, sizeof(JobDev) * capacity));
+    MG_CUDA(cudaMemset(d_jobs_, 0, sizeof(JobDev) * capacity));
+    MG_CUDA(cudaMalloc(&d_err_, sizeof(int)));
+    MG_CUDA(cudaMemset(d_err_, 0, sizeof(int)));
+    MG_CUDA(cudaMalloc(&d_diag_part_, sizeof(double2) * 3 * kDiagBlocks));
+    MG_CUDA(cudaMalloc(&d_diag_max_, sizeof(double) * kDiagBlocks));
+    MG_CUDA(cudaMalloc(&d_diag_bad_, sizeof(double) * kDiagBlocks));
+    MG_CUDA(cudaMalloc(&d_diag_, sizeof(Diag)));
+    MG_CUDA(cudaHostAlloc(&h_diag_, sizeof(Diag), cudaHostAllocDefault));
+    MG_CUDA(cudaHostAlloc(&h_state_, sizeof(JobDev), cudaHostAllocDefault));
+    for (int s = capacity - 1; s >= 0; --s) free_slots_.push_back(s);
+    return MG_OK;
+}
+
+int Engine::add_job(const mg_ch_params& p, long long target, Job** out)
+{
+    std::unique_ptr<Job> j(new Job);
+    j->p = p;
+    MG_TRY(make_geometry(p, &j->g));
+    if (free_slots_.empty()) return fail(MG_ENOMEM, "no free job slot (capacity %d)", capacity_);
+    MG_CUDA(cudaSetDevice(device));
+    j->tiling = default_tiling(j->g, info, device);
+    MG_TRY(plan_tiling(j->g, j->tiling, info, &j->plan));
+    if (j->p.mass_correct && !j->plan.tma_ok)
+        return fail(MG_EINVAL, "mass_correct needs a shape the tiled kernel takes (nx multiple of %d)", 32);
+    j->target = target;
+    const size_t bytes = j->g.n * j->g.es;
+    cudaError_t e = cudaMalloc(&j->buf[0], bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&j->buf[1], bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&j->d_tmap, 4 * sizeof(CUtensorMap));
+    if (e == cudaSuccess) e = cudaMalloc(&j->d_partial, sizeof(double2) * std::max(j->plan.nitems, 1));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(j->buf[0]);
+        cudaFree(j->buf[1]);
+        cudaFree(j->d_tmap);
+        cudaFree(j->d_partial);
+        return fail(e == cudaErrorMemoryAllocation ? MG_ENOMEM : MG_ECUDA, "allocating %zu bytes: %s", 2 * bytes,
+                    cudaGetErrorString(e));
+    }
+    if (j->plan.tma_ok) {
+        CUtensorMap maps[4];
+        int rc = encode_maps(*j, maps);
+        if (rc == MG_OK) {
+            cudaError_t ce = cudaMemcpy(j->d_tmap, maps, sizeof maps, cudaMemcpyHostToDevice);
+            if (ce != cudaSuccess) rc = fail(MG_ECUDA, "copying tensor maps: %s", cudaGetErrorString(ce));
+        }
+        if (rc != MG_OK) {
+            cudaFree(j->buf[0]);
+            cudaFree(j->buf[1]);
+            cudaFree(j->d_tmap);
+            cudaFree(j->d_partial);
+            return rc;
+        }
+    }
+    j->slot = free_slots_.back();
+    free_slots_.pop_back();
+    JobDev jd;
+    fill_jobdev(*j, &jd);
+    MG_CUDA(cudaMemcpy(d_jobs_ + j->slot, &jd, sizeof jd, cudaMemcpyHostToDevice));
+    jobs.push_back(j.get());
+    dirty_ = true;
+    *out = j.release();
+    return MG_OK;
+}
+
+void Engine::remove_job(Job* j)
+{
+    auto it = std::find(jobs.begin(), jobs.end(), j);
+    if (it == jobs.end()) return;
+    jobs.erase(it);
+    cudaFree(j->buf[0]);
+    cudaFree(j->buf[1]);
+    cudaFree(j->d_tmap);
+    cudaFree(j->d_partial);
+    free_slots_.push_back(j->slot);
+    delete j;
+    dirty_ = true;
+}
+
+int Engine::set_tiling(Job* j, const mg_tiling& t)
+{
+    TilePlan pl;
+    MG_TRY(plan_tiling(j->g, t, info, &pl));
+    if (j->p.mass_correct && !pl.tma_ok) return fail(MG_EINVAL, "mass_correct needs the tiled kernel");
+    MG_CUDA(cudaStreamSynchronize(stream));
+    double2* part = nullptr;
+    MG_CUDA(cudaMalloc(&part, sizeof(double2) * std::max(pl.nitems, 1)));
+    const mg_tiling old = j->tiling;
+    const TilePlan old_plan = j->plan;
+    j->tiling = t;
+    j->plan = pl;
+    if (pl.tma_ok) {
+        // new maps at a new address: a launch never sees a map rewritten in place
+        CUtensorMap maps[4];
+        CUtensorMap* d_new = nullptr;
+        int rc = encode_maps(*j, maps);
+        if (rc == MG_OK) {
+            cudaError_t e = cudaMalloc(&d_new, sizeof maps);
+            if (e == cudaSuccess) e = cudaMemcpy(d_new, maps, sizeof maps, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) rc = fail(MG_ECUDA, "tensor maps: %s", cudaGetErrorString(e));
+        }
+        if (rc != MG_OK) {
+            j->tiling = old;
+            j->plan = old_plan;
+            cudaFree(d_new);
+            cudaFree(part);
+            return rc;
+        }
+        cudaFree(j->d_tmap);
+        j->d_tmap = d_new;
+    }
+    cudaFree(j->d_partial);
+    j->d_partial = part;
+    // rewrite the static part of the slot, keep the mutable state
+    MG_TRY(read_state(j, h_state_));
+    JobDev jd;
+    fill_jobdev(*j, &jd);
+    jd.delta = h_state_->delta;
+    jd.mass_target = h_state_->mass_target;
+    jd.mass_last = h_state_->mass_last;
+    jd.step = h_state_->step;
+    jd.target = h_state_->target;
+    jd.err = h_state_->err;
+    MG_CUDA(cudaMemcpy(d_jobs_ + j->slot, &jd, sizeof jd, cudaMemcpyHostToDevice));
+    dirty_ = true;
+    return MG_OK;
+}
+
+void Engine::free_groups()
+{
+    for (Group& g : groups_) {
+        cudaFree(g.d_item_begin);
+        cudaFree(g.d_slot);
+    }
+    groups_.clear();
+}
+
+void Engine::drop_graphs()
+{
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+}
+
+int Engine::rebuild()
+{
+    MG_CUDA(cudaStreamSynchronize(stream));
+    drop_graphs();
+    free_groups();
+    // one launch per (precision, flat, nbuf) class; generic jobs separately
+    std::map<int, Group> by_key;
+    for (Job* j : jobs) {
+        if (!j->plan.tma_ok) {
+            Group g;
+            g.generic = true;
+            g.fp32 = j->g.es == 4;
+            g.jobs.push_back(j);
+            groups_.push_back(g);
+            continue;
+        }
+        const int key = (j->g.es == 4 ? 1 : 0) | (j->g.flat ? 2 : 0) | (j->tiling.nbuf == 3 ? 4 : 0);
+        Group& g = by_key[key];
+        g.fp32 = j->g.es == 4;
+        g.flat = j->g.flat;
+        g.nbuf = j->tiling.nbuf;
+        g.jobs.push_back(j);
+    }
+    for (auto& kv : by_key) groups_.push_back(kv.second);
+    for (Group& g : groups_) {
+        if (g.generic) continue;
+        std::vector<int> begin, slot;
+        int items = 0;
+        for (Job* j : g.jobs) {
+            begin.push_back(items);
+            slot.push_back(j->slot);
+            items += j->plan.nitems;
+            g.block = std::max(g.block, j->plan.block);
+            g.cplane = std::max(g.cplane, j->plan.cplane);
+            g.mplane = std::max(g.mplane, j->plan.mplane);
+        }
+        begin.push_back(items);
+        g.nitems = items;
+        const int es = g.fp32 ? 4 : 8;
+        const size_t head = (sizeof(SmemHead) + 127) / 128 * 128 + 128;  // + alignment slack
+        g.smem = head + (size_t)g.nbuf * g.cplane * es + (size_t)3 * g.mplane * es;
+        if (g.smem > info.smem_optin) return fail(MG_EINVAL, "batch group needs %zu bytes of shared memory", g.smem);
+        int occ = 1;
+        MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_kernel(g.fp32, g.flat, g.nbuf), g.block,
+                                                              g.smem));
+        occ = std::max(occ, 1);
+        g.grid = std::min(items, info.sms * occ);
+        MG_CUDA(cudaMalloc(&g.d_item_begin, sizeof(int) * begin.size()));
+        MG_CUDA(cudaMalloc(&g.d_slot, sizeof(int) * slot.size()));
+        MG_CUDA(cudaMemcpy(g.d_item_begin, begin.data(), sizeof(int) * begin.size(), cudaMemcpyHostToDevice));
+        MG_CUDA(cudaMemcpy(g.d_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice));
+    }
+    dirty_ = false;
+    return MG_OK;
+}
+
+// Polls of a TMA completion barrier before the kernel gives up (reads the
+// environment on every call so tests can shorten it).
+static long long spin_limit()
+{
+    const char* e = std::getenv("MG_SPIN_LIMIT");
+    const long long v = e ? std::atoll(e) : 0;
+    return v > 0 ? v : (1LL << 22);
+}
+
+// Test hook for the bounded device waits: MG_FAULT_TX_EXTRA=<bytes> makes
+// every plane's barrier expect more bytes than its copies deliver, so each
+// wait runs out of polls and the kernel reports DEV_TMA_TIMEOUT.
+static uint32_t fault_tx_extra()
+{
+    const char* e = std::getenv("MG_FAULT_TX_EXTRA");
+    const long long v = e ? std::atoll(e) : 0;
+    return v > 0 && v < 4096 ? (uint32_t)v : 0u;
+}
+
+int Engine::launch_once()
+{
+    for (Group& g : groups_) {
+        if (g.generic) {
+            for (Job* j : g.jobs) {
+                const unsigned blocks = (unsigned)((j->g.n + 255) / 256);
+                if (g.fp32) ch_step_generic_kernel<float><<<blocks, 256, 0, stream>>>(d_jobs_ + j->slot);
+                else ch_step_generic_kernel<double><<<blocks, 256, 0, stream>>>(d_jobs_ + j->slot);
+                ch_step_generic_finish<<<1, 32, 0, stream>>>(d_jobs_ + j->slot);
+            }
+            continue;
+        }
+        StepArgs a;
+        a.jobs = d_jobs_;
+        a.job_slot = g.d_slot;
+        a.item_begin = g.d_item_begin;
+        a.njobs = (int)g.jobs.size();
+        a.nitems = g.nitems;
+        a.cplane = g.cplane;
+        a.mplane = g.mplane;
+        a.spin_limit = spin_limit();
+        a.err = d_err_;
+        a.tx_extra = fault_tx_extra();
+        step_kernel(g.fp32, g.flat, g.nbuf)<<<g.grid, g.block, g.smem, stream>>>(a);
+    }
+    MG_CUDA(cudaGetLastError());
+    return MG_OK;
+}
+
+int Engine::graph_for(int k, cudaGraphExec_t* out)
+{
+    auto it = graphs_.find(k);
+    if (it != graphs_.end()) {
+        *out = it->second;
+        return MG_OK;
+    }
+    cudaGraph_t graph;
+    MG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    int rc = MG_OK;
+    for (int i = 0; i < k && rc == MG_OK; ++i) rc = launch_once();
+    cudaError_t e = cudaStreamEndCapture(stream, &graph);
+    if (rc != MG_OK) {
+        if (e == cudaSuccess) cudaGraphDestroy(graph);
+        return rc;
+    }
+    MG_CUDA(e);
+    cudaGraphExec_t exec;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    MG_CUDA(e);
+    graphs_[k] = exec;
+    *out = exec;
+    return MG_OK;
+}
+
+static int graph_steps()
+{
+    static int v = [] {
+        const char* e = std::getenv("MG_GRAPH_STEPS");
+        return e ? std::max(0, std::atoi(e)) : 50;
+    }();
+    return v;
+}
+
+int Engine::enqueue_steps(int nsteps)
+{
+    if (nsteps < 0) return fail(MG_EINVAL, "nsteps must be >= 0");
+    MG_CUDA(cudaSetDevice(device));
+    if (dirty_) MG_TRY(rebuild());
+    if (jobs.empty()) return MG_OK;
+    const int gk = graph_steps();
+    while (nsteps > 0) {
+        if (gk >= 2 && nsteps >= 2) {
+            const int k = std::min(nsteps, gk);
+            cudaGraphExec_t ex;
+            MG_TRY(graph_for(k, &ex));
+            MG_CUDA(cudaGraphLaunch(ex, stream));
+            nsteps -= k;
+        } else {
+            MG_TRY(launch_once());
+            nsteps -= 1;
+        }
+    }
+    return MG_OK;
+}
+
+int Engine::sync(long long timeout_us)
+{
+    MG_CUDA(cudaSetDevice(device));
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(stream);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorNotReady) MG_CUDA(e);
+        if (timeout_us >= 0) {
+            const auto us =
+                std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0).count();
+            if (us > timeout_us) return fail(MG_ETIMEOUT, "GPU work not finished after %lld us", timeout_us);
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+    int err = 0;
+    MG_CUDA(cudaMemcpy(&err, d_err_, sizeof err, cudaMemcpyDeviceToHost));
+    if (err != DEV_OK) return fail(MG_EDEVICE, "a step kernel reported device error %d (TMA wait ran out)", err);
+    return MG_OK;
+}
+
+int Engine::read_state(Job* j, JobDev* out)
+{
+    MG_CUDA(cudaSetDevice(device));
+    MG_CUDA(cudaMemcpyAsync(h_state_, d_jobs_ + j->slot, sizeof(JobDev), cudaMemcpyDeviceToHost, stream));
+    MG_CUDA(cudaStreamSynchronize(stream));
+    *out = *h_state_;
+    return MG_OK;
+}
+
+int Engine::ensure_stage(size_t n)
+{
+    if (stage_n_ >= n) return MG_OK;
+    cudaFree(d_stage_);
+    d_stage_ = nullptr;
+    stage_n_ = 0;
+    cudaError_t e = cudaMalloc(&d_stage_, n * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(MG_ENOMEM, "staging buffer of %zu doubles: %s", n, cudaGetErrorString(e));
+    }
+    stage_n_ = n;
+    return MG_OK;
+}
+
+int Engine::upload(Job* j, const double* host, long long target)
+{
+    if (!host) return fail(MG_EINVAL, "null field");
+    MG_CUDA(cudaSetDevice(device));
+    if (j->g.es == 8) {
+        MG_CUDA(cudaMemcpyAsync(j->buf[0], host, j->g.n * 8, cudaMemcpyHostToDevice, stream));
+    } else {
+        MG_TRY(ensure_stage(j->g.n));
+        MG_CUDA(cudaMemcpyAsync(d_stage_, host, j->g.n * 8, cudaMemcpyHostToDevice, stream));
+        ch_convert<double, float><<<4 * info.sms, 256, 0, stream>>>(d_stage_, static_cast<float*>(j->buf[0]), j->g.n);
+    }
+    j->target = target;
+    ch_job_reset<<<1, 32, 0, stream>>>(d_jobs_ + j->slot, target < 0 ? LLONG_MAX : target);
+    if (j->g.es == 4) {
+        ch_mass_partial<float><<<kDiagBlocks, kDiagThreads, 0, stream>>>(d_jobs_ + j->slot, d_diag_part_);
+        ch_mass_final<<<1, 256, 0, stream>>>(d_diag_part_, kDiagBlocks, d_jobs_ + j->slot);
+    }
+    MG_CUDA(cudaGetLastError());
+    return MG_OK;
+}
+
+int Engine::to_double(Job* j, double* d_dst)
+{
+    MG_TRY(read_state(j, h_state_));
+    const void* cur = j->buf[h_state_->step & 1];
+    if (j->g.es == 8) {
+        MG_CUDA(cudaMemcpyAsync(d_dst, cur, j->g.n * 8, cudaMemcpyDeviceToDevice, stream));
+    } else {
+        ch_convert<float, double><<<4 * info.sms, 256, 0, stream>>>(static_cast<const float*>(cur), d_dst, j->g.n);
+        MG_CUDA(cudaGetLastError());
+    }
+    return MG_OK;
+}
+
+int Engine::download(Job* j, double* host)
+{
+    if (!host) return fail(MG_EINVAL, "null field");
+    MG_TRY(sync(-1));
+    MG_TRY(read_state(j, h_state_));
+    const void* cur = j->buf[h_state_->step & 1];
+    if (j->g.es == 8) {
+        MG_CUDA(cudaMemcpyAsync(host, cur, j->g.n * 8, cudaMemcpyDeviceToHost, stream));
+    } else {
+        MG_TRY(ensure_stage(j->g.n));
+        ch_convert<float, double><<<4 * info.sms, 256, 0, stream>>>(static_cast<const float*>(cur), d_stage_, j->g.n);
+        MG_CUDA(cudaMemcpyAsync(host, d_stage_, j->g.n * 8, cudaMemcpyDeviceToHost, stream));
+    }
+    MG_CUDA(cudaStreamSynchronize(stream));
+    return MG_OK;
+}
+
+int Engine::diagnostics(Job* j, mg_ch_stats* out)
+{
+    if (!out) return fail(MG_EINVAL, "null stats");
+    MG_TRY(sync(-1));
+    const Geometry& g = j->g;
+    if (g.es == 8)
+        ch_diag_partial<double><<<kDiagBlocks, kDiagThreads, 0, stream>>>(d_jobs_ + j->slot, g.lsx, g.lsy, g.lsz,
+                                                                           d_diag_part_, d_diag_max_, d_diag_bad_);
+    else
+        ch_diag_partial<float><<<kDiagBlocks, kDiagThreads, 0, stream>>>(d_jobs_ + j->slot, g.lsx, g.lsy, g.lsz,
+                                                                          d_diag_part_, d_diag_max_, d_diag_bad_);
+    ch_diag_final<<<1, 256, 0, stream>>>(d_diag_part_, d_diag_max_, d_diag_bad_, kDiagBlocks, g.lsx * g.lsy * g.lsz,
+                                         d_diag_);
+    MG_CUDA(cudaGetLastError());
+    MG_CUDA(cudaMemcpyAsync(h_diag_, d_diag_, sizeof(Diag), cudaMemcpyDeviceToHost, stream));
+    MG_TRY(read_state(j, h_state_));  // syncs the stream
+    out->mass = h_diag_->mass;
+    out->energy = h_diag_->energy;
+    out->abs_mass = h_diag_->abs_mass;
+    out->max_abs = h_diag_->max_abs;
+    out->nonfinite = (long long)h_diag_->nonfinite;
+    out->step = h_state_->step;
+    if (out->nonfinite > 0) return fail(MG_ENONFINITE, "%lld sites are NaN or Inf", out->nonfinite);
+    return MG_OK;
+}
+
+int Engine::nitems_total() const
+{
+    int s = 0;
+    for (const Group& g : groups_) s += g.generic ? (int)g.jobs.size() : g.nitems;
+    return s;
+}
+int Engine::nctas_total() const
+{
+    int s = 0;
+    for (const Group& g : groups_) s += g.generic ? 0 : g.grid;
+    return s;
+}
+int Engine::nlaunch_per_step() const
+{
+    int s = 0;
+    for (const Group& g : groups_) s += g.generic ? 2 * (int)g.jobs.size() : 1;
+    return s;
+}
+
+// ------------------------------------------------------ structure factor
+// Bins |F|^2/N of the half spectrum with Hermitian weights; k = 0 excluded.
+__global__ void sf_bin_kernel(const cufftDoubleComplex* __restrict__ F, int nx, int ny, int nz, double spx,
+                              double spy, double spz, double dk, int nbins, double inv_n, double* __restrict__ acc)
+{
+    const int hx = nx / 2 + 1;
+    const size_t total = (size_t)hx * ny * nz;
+    const double two_pi = 6.283185307179586476925286766559;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(i % hx);
+        const int iy = (int)((i / hx) % ny);
+        const int iz = (int)(i / ((size_t)hx * ny));
+        const int fy = iy <= ny / 2 ? iy : iy - ny;
+        const int fz = iz <= nz / 2 ? iz : iz - nz;
+        const double kx = two_pi * ix / (nx * spx), ky = two_pi * fy / (ny * spy), kz = two_pi * fz / (nz * spz);
+        const double kk = sqrt(kx * kx + ky * ky + kz * kz);
+        if (kk <= 0.0) continue;
+        const int b = (int)floor(kk / dk);
+        if (b >= nbins) continue;
+        const double w = (ix == 0 || (nx % 2 == 0 && ix == nx / 2)) ? 1.0 : 2.0;
+        const double s = (F[i].x * F[i].x + F[i].y * F[i].y) * inv_n;
+        atomicAdd(acc + 4 * b + 0, w);
+        atomicAdd(acc + 4 * b + 1, w * kk);
+        atomicAdd(acc + 4 * b + 2, w * s);
+        atomicAdd(acc + 4 * b + 3, w * kk * s);
+    }
+}
+
+int Engine::structure_factor(Job* j, int nbins, double* k, double* S, double* k1)
+{
+    if (nbins < 1 || !k || !S || !k1) return fail(MG_EINVAL, "structure_factor: bad arguments");
+    MG_TRY(sync(-1));
+    const mg_ch_params& p = j->p;
+    const int nx = p.nx, ny = p.ny, nz = p.nz;
+    const size_t n = j->g.n;
+    const size_t nc = (size_t)(nx / 2 + 1) * ny * nz;
+    MG_TRY(ensure_stage(n));
+    MG_TRY(to_double(j, d_stage_));
+    cufftDoubleComplex* F = nullptr;
+    double* acc = nullptr;
+    MG_CUDA(cudaMalloc(&F, nc * sizeof(cufftDoubleComplex)));
+    cudaError_t e = cudaMalloc(&acc, 4 * nbins * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaFree(F);
+        MG_CUDA(e);
+    }
+    cufftHandle plan;
+    cufftResult fr;
+    if (nz > 1) fr = cufftPlan3d(&plan, nz, ny, nx, CUFFT_D2Z);
+    else if (ny > 1) fr = cufftPlan2d(&plan, ny, nx, CUFFT_D2Z);
+    else fr = cufftPlan1d(&plan, nx, CUFFT_D2Z, 1);
+    const bool planned = fr == CUFFT_SUCCESS;
+    int rc = MG_OK;
+    if (!planned) rc = fail(MG_ECUDA, "cufftPlan failed (%d)", (int)fr);
+    if (rc == MG_OK) {
+        cufftSetStream(plan, stream);
+        fr = cufftExecD2Z(plan, d_stage_, F);
+        if (fr != CUFFT_SUCCESS) rc = fail(MG_ECUDA, "cufftExecD2Z failed (%d)", (int)fr);
+    }
+    std::vector<double> h(4 * nbins);
+    if (rc == MG_OK) {
+        const double L = std::max({nx * p.dx, ny * p.dy, nz * p.dz});
+        const double dk = 6.283185307179586476925286766559 / L;
+        cudaMemsetAsync(acc, 0, 4 * nbins * sizeof(double), stream);
+        sf_bin_kernel<<<8 * info.sms, 256, 0, stream>>>(F, nx, ny, nz, p.dx, p.dy, p.dz, dk, nbins, 1.0 / (double)n,
+                                                        acc);
+        cudaError_t ce = cudaMemcpyAsync(h.data(), acc, 4 * nbins * sizeof(double), cudaMemcpyDeviceToHost, stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(stream);
+        if (ce != cudaSuccess) rc = fail(MG_ECUDA, "structure factor: %s", cudaGetErrorString(ce));
+        double num = 0, den = 0;
+        for (int b = 0; b < nbins && rc == MG_OK; ++b) {
+            const double cnt = h[4 * b], ks = h[4 * b + 1], ss = h[4 * b + 2], kss = h[4 * b + 3];
+            k[b] = cnt > 0 ? ks / cnt : (b + 0.5) * dk;
+            S[b] = cnt > 0 ? ss / cnt : 0.0;
+            num += kss;
+            den += ss;
+        }
+        *k1 = den > 0 ? num / den : 0.0;
+    }
+    if (planned) cufftDestroy(plan);
+    cudaFree(F);
+    cudaFree(acc);
+    return rc;
+}
+
+}  // namespace mg

@@ -1,0 +1,155 @@
+// Host-side engine behind the C ABI: owns device memory, job slots, the
+// launch groups of the fused step kernel and their CUDA graphs.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ch_types.h"
+#include "mesogpu.h"
+
+namespace mg {
+
+// ---- error reporting (thread-local message, C-ABI return codes)
+int fail(int code, const char* fmt, ...);
+void clear_error();
+const char* last_error();
+
+#define MG_CUDA(call)                                                                                    \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            return ::mg::fail(MG_ECUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                              __LINE__);                                                                 \
+    } while (0)
+
+#define MG_TRY(call)                 \
+    do {                             \
+        int rc_ = (call);            \
+        if (rc_ != MG_OK) return rc_; \
+    } while (0)
+
+struct DevInfo {
+    int sms = 0;
+    size_t smem_optin = 0;
+    size_t total_mem = 0;
+    int major = 0, minor = 0;
+};
+int device_info(int device, DevInfo* out);
+
+// Geometry of one job as the kernels see it.
+struct Geometry {
+    int lnx = 0, lny = 0, lnz = 0;  // logical dims (2-D runs as nx, 1, ny)
+    bool flat = false;
+    double lsx = 1, lsy = 1, lsz = 1;  // logical spacing
+    int perx = 1, pery = 1, perz = 1;  // logical periodic flags
+    size_t n = 0;
+    int es = 8;  // element size
+};
+int make_geometry(const mg_ch_params& p, Geometry* g);
+int validate_params(const mg_ch_params& p);
+
+// Resource needs of a tiling on a geometry.
+struct TilePlan {
+    bool tma_ok = false;  // the tiled kernel can take this shape
+    int block = 0;        // threads used by a tile
+    int cplane = 0, mplane = 0;
+    size_t smem = 0;
+    int ntile = 0, nitems = 0;
+};
+int plan_tiling(const Geometry& g, const mg_tiling& t, const DevInfo& d, TilePlan* out);
+bool tma_shape_ok(const Geometry& g);
+mg_tiling default_tiling(const Geometry& g, const DevInfo& d, int device);
+std::string tune_key(const Geometry& g);
+bool tune_lookup(const std::string& key, mg_tiling* t);
+void tune_store(const std::string& key, const mg_tiling& t, double ms);
+
+struct Job {
+    mg_ch_params p{};
+    Geometry g;
+    mg_tiling tiling{};
+    TilePlan plan;
+    void* buf[2] = {nullptr, nullptr};
+    CUtensorMap* d_tmap = nullptr;  // 4 maps
+    double2* d_partial = nullptr;
+    int slot = -1;
+    long long target = -1;  // device step target (-1: unbounded)
+    size_t device_bytes() const;
+};
+
+class Engine {
+   public:
+    Engine() = default;
+    ~Engine();
+    int init(int device, int capacity);
+
+    // job lifetime: allocate buffers + maps, take a slot
+    int add_job(const mg_ch_params& p, long long target, Job** out);
+    void remove_job(Job* j);  // frees everything of the job (caller synced)
+    int set_tiling(Job* j, const mg_tiling& t);
+
+    int upload(Job* j, const double* host, long long target);  // resets step
+    int download(Job* j, double* host);                         // syncs
+    int diagnostics(Job* j, mg_ch_stats* out);                  // syncs
+    int structure_factor(Job* j, int nbins, double* k, double* S, double* k1);
+    int enqueue_steps(int nsteps);  // all jobs, one launch group set per step
+    int sync(long long timeout_us);
+    int read_state(Job* j, JobDev* out);  // syncs; mutable state of the slot
+
+    int nitems_total() const;
+    int nctas_total() const;
+    int nlaunch_per_step() const;
+
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    DevInfo info;
+    std::vector<Job*> jobs;
+
+   private:
+    struct Group {
+        bool fp32 = false, flat = false, generic = false;
+        int nbuf = 4;
+        std::vector<Job*> jobs;
+        int nitems = 0, grid = 0, block = 0;
+        size_t smem = 0;
+        int cplane = 0, mplane = 0;
+        int* d_item_begin = nullptr;
+        int* d_slot = nullptr;
+    };
+    int rebuild();
+    void free_groups();
+    int launch_once();
+    int graph_for(int k, cudaGraphExec_t* out);
+    void drop_graphs();
+    int to_double(Job* j, double* d_dst);   // current field -> device doubles
+    int ensure_stage(size_t n);
+
+    int capacity_ = 0;
+    JobDev* d_jobs_ = nullptr;
+    int* d_err_ = nullptr;
+    std::vector<int> free_slots_;
+    std::vector<Group> groups_;
+    bool dirty_ = true;
+    std::map<int, cudaGraphExec_t> graphs_;
+    double* d_stage_ = nullptr;  // conversion staging (doubles)
+    size_t stage_n_ = 0;
+    double2* d_diag_part_ = nullptr;
+    double* d_diag_max_ = nullptr;
+    double* d_diag_bad_ = nullptr;
+    Diag* d_diag_ = nullptr;
+    Diag* h_diag_ = nullptr;  // pinned
+    JobDev* h_state_ = nullptr;  // pinned
+};
+
+// kernel table
+using StepKernel = void (*)(StepArgs);
+StepKernel step_kernel(bool fp32, bool flat, int nbuf);
+int prepare_kernels(const DevInfo& d);
+
+}  // namespace mg

@@ -1,0 +1,315 @@
+// Continuous-batching server over the step engine (mg_server_* in
+// include/mesogpu.h).
+//
+// A worker thread owns one Engine.  Each tick it
+//   1. admits queued jobs, oldest first, that fit the HBM budget and a free
+//      slot (first fit: a large job at the head does not block small ones);
+//   2. enqueues k steps for every admitted job together -- one fused launch
+//      per precision class per step, all jobs' tiles in the same persistent
+//      grid -- where k is the fewest steps any admitted job still needs
+//      (capped), so finished jobs retire promptly;
+//   3. retires jobs that reached their step count: downloads the field and
+//      diagnostics, frees their memory, records the latency.
+// Per-job arithmetic does not depend on which other jobs share a launch:
+// each job's decomposition and reduction trees depend on its own shape only.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "engine.h"
+
+using mg::fail;
+using Clock = std::chrono::steady_clock;
+
+namespace {
+
+struct ServerJob {
+    long long id = 0;
+    mg_ch_params p{};
+    std::vector<double> ic;
+    long long nsteps = 0;
+    long long done_steps = 0;
+    int state = MG_JOB_QUEUED;
+    mg::Job* job = nullptr;
+    size_t bytes = 0;
+    Clock::time_point t_submit, t_done;
+    std::vector<double> result;
+    mg_ch_stats stats{};
+    std::string error;
+};
+
+}  // namespace
+
+struct mg_server {
+    mg::Engine eng;
+    double budget = 0;
+    int max_inflight = 0;
+    int steps_per_tick = 0;
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<ServerJob*> queue;
+    std::vector<ServerJob*> running;
+    std::map<long long, std::unique_ptr<ServerJob>> jobs;
+    long long next_id = 1;
+    bool stopping = false;
+    size_t in_use = 0, peak = 0;
+    long long submitted = 0, completed = 0, failed = 0;
+    std::vector<double> latencies_ms;
+    bool have_first = false;
+    Clock::time_point t_first, t_last;
+    double site_updates = 0;
+
+    void run();
+    void admit_locked();
+    void retire(ServerJob* sj, bool ok, const char* why);
+};
+
+static size_t job_bytes(const mg_ch_params& p)
+{
+    const size_t n = (size_t)p.nx * p.ny * p.nz;
+    return 2 * n * (p.precision == MG_FP32 ? 4 : 8) + (1 << 16);
+}
+
+void mg_server::admit_locked()
+{
+    for (auto it = queue.begin(); it != queue.end();) {
+        if ((int)running.size() >= max_inflight) break;
+        ServerJob* sj = *it;
+        if ((double)(in_use + sj->bytes) > budget) {
+            ++it;
+            continue;
+        }
+        mg::Job* j = nullptr;
+        int rc = eng.add_job(sj->p, sj->nsteps, &j);
+        if (rc == MG_OK) rc = eng.upload(j, sj->ic.data(), sj->nsteps);
+        if (rc != MG_OK) {
+            if (j) eng.remove_job(j);
+            sj->state = MG_JOB_FAILED;
+            sj->error = mg::last_error();
+            sj->t_done = Clock::now();
+            ++failed;
+            it = queue.erase(it);
+            cv_done.notify_all();
+            continue;
+        }
+        std::vector<double>().swap(sj->ic);
+        sj->job = j;
+        sj->state = MG_JOB_RUNNING;
+        in_use += sj->bytes;
+        peak = std::max(peak, in_use);
+        running.push_back(sj);
+        it = queue.erase(it);
+    }
+}
+
+void mg_server::retire(ServerJob* sj, bool ok, const char* why)
+{
+    if (ok) {
+        sj->result.resize((size_t)sj->p.nx * sj->p.ny * sj->p.nz);
+        int rc = eng.download(sj->job, sj->result.data());
+        if (rc == MG_OK) {
+            rc = eng.diagnostics(sj->job, &sj->stats);
+            if (rc == MG_ENONFINITE) rc = MG_OK;  // reported in stats.nonfinite
+        }
+        if (rc != MG_OK) {
+            ok = false;
+            why = mg::last_error();
+        }
+    }
+    eng.remove_job(sj->job);
+    sj->job = nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    in_use -= sj->bytes;
+    sj->t_done = Clock::now();
+    t_last = sj->t_done;
+    if (ok) {
+        sj->state = MG_JOB_DONE;
+        ++completed;
+        latencies_ms.push_back(std::chrono::duration<double, std::milli>(sj->t_done - sj->t_submit).count());
+        site_updates += (double)sj->p.nx * sj->p.ny * sj->p.nz * (double)sj->nsteps;
+    } else {
+        sj->state = MG_JOB_FAILED;
+        sj->error = why ? why : "failed";
+        ++failed;
+    }
+    running.erase(std::find(running.begin(), running.end(), sj));
+    cv_done.notify_all();
+}
+
+void mg_server::run()
+{
+    cudaSetDevice(eng.device);
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lock(mu);
+            admit_locked();
+            while (running.empty()) {
+                if (stopping && queue.empty()) return;
+                cv_work.wait_for(lock, std::chrono::milliseconds(20));
+                admit_locked();
+            }
+        }
+        long long k = steps_per_tick;
+        for (ServerJob* sj : running) k = std::min(k, sj->nsteps - sj->done_steps);
+        k = std::max(k, 1LL);
+        int rc = eng.enqueue_steps((int)k);
+        if (rc == MG_OK) rc = eng.sync(600LL * 1000 * 1000);
+        std::vector<ServerJob*> snapshot = running;
+        if (rc != MG_OK) {
+            const std::string why = mg::last_error();
+            for (ServerJob* sj : snapshot) retire(sj, false, why.c_str());
+            continue;
+        }
+        for (ServerJob* sj : snapshot) {
+            sj->done_steps = std::min(sj->nsteps, sj->done_steps + k);
+            if (sj->done_steps >= sj->nsteps) retire(sj, true, nullptr);
+        }
+    }
+}
+
+extern "C" {
+
+int mg_server_create(int device, double hbm_budget_gb, int max_jobs_in_flight, int steps_per_tick,
+                     mg_server_t** out)
+{
+    mg::clear_error();
+    if (!out || hbm_budget_gb <= 0 || max_jobs_in_flight < 1) return fail(MG_EINVAL, "bad server arguments");
+    *out = nullptr;
+    std::unique_ptr<mg_server> s(new (std::nothrow) mg_server);
+    if (!s) return fail(MG_ENOMEM, "host allocation failed");
+    MG_TRY(s->eng.init(device, max_jobs_in_flight));
+    s->budget = hbm_budget_gb * 1e9;
+    s->max_inflight = max_jobs_in_flight;
+    s->steps_per_tick = steps_per_tick > 0 ? steps_per_tick : 100;
+    mg_server* raw = s.get();
+    s->worker = std::thread([raw] { raw->run(); });
+    *out = s.release();
+    return MG_OK;
+}
+
+int mg_server_submit(mg_server_t* s, const mg_ch_params* params, const double* ic_host, long long nsteps,
+                     long long* job_id)
+{
+    mg::clear_error();
+    if (!s || !params || !ic_host || nsteps < 1) return fail(MG_EINVAL, "bad submit arguments");
+    mg::Geometry g;
+    MG_TRY(mg::make_geometry(*params, &g));
+    std::unique_ptr<ServerJob> sj(new (std::nothrow) ServerJob);
+    if (!sj) return fail(MG_ENOMEM, "host allocation failed");
+    sj->p = *params;
+    sj->nsteps = nsteps;
+    sj->bytes = job_bytes(*params);
+    if ((double)sj->bytes > s->budget)
+        return fail(MG_ENOMEM, "job needs %.3f GB, above the server budget %.3f GB", sj->bytes / 1e9, s->budget / 1e9);
+    sj->ic.assign(ic_host, ic_host + g.n);
+    sj->t_submit = Clock::now();
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (s->stopping) return fail(MG_EINVAL, "server is stopping");
+    sj->id = s->next_id++;
+    if (!s->have_first) {
+        s->have_first = true;
+        s->t_first = sj->t_submit;
+    }
+    if (job_id) *job_id = sj->id;
+    s->queue.push_back(sj.get());
+    s->jobs[sj->id] = std::move(sj);
+    ++s->submitted;
+    s->cv_work.notify_all();
+    return MG_OK;
+}
+
+int mg_server_poll(mg_server_t* s, long long job_id, int* state)
+{
+    mg::clear_error();
+    if (!s || !state) return fail(MG_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->jobs.find(job_id);
+    if (it == s->jobs.end()) return fail(MG_ENOTFOUND, "unknown job %lld", job_id);
+    *state = it->second->state;
+    return MG_OK;
+}
+
+int mg_server_result(mg_server_t* s, long long job_id, long long timeout_us, double* field_out, mg_ch_stats* stats)
+{
+    mg::clear_error();
+    if (!s) return fail(MG_EINVAL, "null handle");
+    std::unique_lock<std::mutex> lock(s->mu);
+    auto it = s->jobs.find(job_id);
+    if (it == s->jobs.end()) return fail(MG_ENOTFOUND, "unknown job %lld", job_id);
+    ServerJob* sj = it->second.get();
+    auto finished = [&] { return sj->state == MG_JOB_DONE || sj->state == MG_JOB_FAILED; };
+    if (timeout_us < 0) s->cv_done.wait(lock, finished);
+    else if (!s->cv_done.wait_for(lock, std::chrono::microseconds(timeout_us), finished))
+        return fail(MG_ETIMEOUT, "job %lld not finished after %lld us", job_id, timeout_us);
+    if (sj->state == MG_JOB_FAILED) {
+        std::string why = sj->error;
+        s->jobs.erase(it);
+        return fail(MG_EDEVICE, "job %lld failed: %s", job_id, why.c_str());
+    }
+    if (field_out) std::copy(sj->result.begin(), sj->result.end(), field_out);
+    if (stats) *stats = sj->stats;
+    s->jobs.erase(it);
+    return MG_OK;
+}
+
+int mg_server_stats_get(mg_server_t* s, mg_server_stats* out)
+{
+    mg::clear_error();
+    if (!s || !out) return fail(MG_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lock(s->mu);
+    mg_server_stats st{};
+    st.submitted = s->submitted;
+    st.completed = s->completed;
+    st.failed = s->failed;
+    st.running = (long long)s->running.size();
+    st.queued = (long long)s->queue.size();
+    if (!s->latencies_ms.empty()) {
+        std::vector<double> v = s->latencies_ms;
+        std::sort(v.begin(), v.end());
+        auto pct = [&](double q) {
+            const double pos = q * (v.size() - 1);
+            const size_t lo = (size_t)pos;
+            const size_t hi = std::min(lo + 1, v.size() - 1);
+            return v[lo] + (v[hi] - v[lo]) * (pos - lo);
+        };
+        st.p50_ms = pct(0.50);
+        st.p99_ms = pct(0.99);
+        double sum = 0;
+        for (double x : v) sum += x;
+        st.mean_ms = sum / v.size();
+    }
+    if (s->have_first && s->completed > 0) {
+        const double wall = std::chrono::duration<double>(s->t_last - s->t_first).count();
+        if (wall > 0) {
+            st.sims_per_hour = s->completed / wall * 3600.0;
+            st.site_updates_per_s = s->site_updates / wall;
+        }
+    }
+    st.hbm_in_use_gb = s->in_use / 1e9;
+    st.hbm_peak_gb = s->peak / 1e9;
+    *out = st;
+    return MG_OK;
+}
+
+void mg_server_destroy(mg_server_t* s)
+{
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stopping = true;
+        s->cv_work.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    delete s;
+}
+
+}  // extern "C"

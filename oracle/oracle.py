@@ -156,10 +156,11 @@ def ref_ic(dims, co, amp, gaussian=False, seed=42) -> np.ndarray:
 # ------------------------------------------------- quantities with no reference
 def structure_factor(c, dims, spacing=(1.0, 1.0, 1.0), nbins=None):
     """Radially binned S(k) = |FFT(c - <c>)|^2 / N and its first-moment
-    wavenumber k1 = sum(k S) / sum(S) over the binned spectrum.
+    wavenumber k1 = sum(|k| S) / sum(S) over every mode in the bins.
 
     Bin b holds |k| in [b*dk, (b+1)*dk) with dk = 2*pi/max(L); the k = 0
-    mode is excluded.  Returns (k_centres, S_binned, counts, k1)."""
+    mode is excluded.  k_centres[b] is the mean |k| and S_binned[b] the mean
+    S of the modes in bin b.  Returns (k_centres, S_binned, counts, k1)."""
     nx, ny, nz = dims
     a = np.asarray(c, dtype=np.float64).reshape(nz, ny, nx)
     f = np.fft.fftn(a - a.mean())
@@ -178,7 +179,8 @@ def structure_factor(c, dims, spacing=(1.0, 1.0, 1.0), nbins=None):
     ksum = np.bincount(b[mask], weights=kk[mask], minlength=nbins)
     kc = np.where(cnt > 0, ksum / np.maximum(cnt, 1), (np.arange(nbins) + 0.5) * dk)
     sbar = np.where(cnt > 0, sb / np.maximum(cnt, 1), 0.0)
-    k1 = float((kc * sbar).sum() / sbar.sum()) if sbar.sum() > 0 else 0.0
+    ks = (kk[mask] * s[mask]).sum()
+    k1 = float(ks / sb.sum()) if sb.sum() > 0 else 0.0
     return kc, sbar, cnt, k1
 
 

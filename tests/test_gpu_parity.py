@@ -1,0 +1,238 @@
+"""GPU path against the checkers, through the C ABI.
+
+FP64: bit-identical to the reference build (golden vectors) and to the C
+restatement at every tiling, boundary condition and spacing.  FP32: within
+the stated tolerances of the FP64 result."""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+
+import mesobasic_b200 as mb
+
+pytestmark = pytest.mark.gpu
+
+
+def params_from(meta, precision="fp64", mass_correct=None):
+    nx, ny, nz = meta["dims"]
+    sx, sy, sz = meta["spacing"]
+    return mb.make_params(nx, ny, nz, meta["dt"], kappa=meta["kap"], M=meta["M"], dx=sx, dy=sy, dz=sz,
+                          bc=tuple(meta["bc"]), precision=precision, mass_correct=mass_correct)
+
+
+def run_gpu(params, ic, nsteps, tiling=None):
+    with mb.CHSim(params) as sim:
+        if tiling is not None:
+            sim.tiling = tiling
+        sim.set_field(ic)
+        sim.step(nsteps)
+        return sim.get_field()
+
+
+@pytest.mark.parametrize("name", golden_cases())
+@pytest.mark.parametrize("path", [0, 1])
+def test_fp64_bit_identical_to_reference_golden(name, path):
+    meta, arr = load_golden(name)
+    p = params_from(meta)
+    with mb.CHSim(p) as sim:
+        if path == 1:
+            t = sim.tiling
+            sim.tiling = (t.ty, t.nchunk, t.nbuf, 1)
+        elif sim.tiling.path != 0:
+            pytest.skip("shape not taken by the tiled kernel")
+        sim.set_field(arr["ic"])
+        done = 0
+        for s in meta["steps"]:
+            sim.step(s - done)
+            done = s
+            out = sim.get_field()
+            assert np.array_equal(out, arr[f"step{s}"]), (name, s, np.abs(out - arr[f"step{s}"]).max())
+
+
+TILED_CASES = [
+    # dims, spacing, bc, M, kap, dt
+    ((64, 48, 40), (1, 1, 1), (1, 1, 1), 1.0, 1.0, 0.005),
+    ((64, 20, 13), (1, 1, 1), (1, 1, 1), 1.0, 1.5, 0.005),
+    ((32, 7, 9), (1, 1, 1), (1, 1, 1), 1.0, 1.0, 0.005),
+    ((96, 16, 12), (1, 1, 1), (0, 0, 0), 1.0, 1.0, 0.004),
+    ((64, 10, 11), (1, 1, 1), (1, 0, 1), 1.0, 1.0, 0.004),
+    ((64, 12, 10), (0.9, 1.1, 1.3), (1, 1, 1), 1.3, 0.8, 0.001),
+    ((512, 6, 5), (1, 1, 1), (1, 1, 1), 1.0, 1.0, 0.005),
+    ((128, 1, 40), (1, 1, 1), (1, 1, 1), 1.0, 1.0, 0.01),
+    ((256, 64, 1), (1, 1, 1), (1, 1, 1), 1.0, 1.0, 0.01),
+    ((64, 33, 1), (0.5, 0.5, 1), (0, 1, 1), 1.0, 1.0, 0.0005),
+]
+
+
+@pytest.mark.parametrize("case", TILED_CASES, ids=lambda c: "x".join(map(str, c[0])))
+def test_fp64_tiled_bit_identical_to_oracle(oracle, case):
+    dims, sp, bc, M, kap, dt = case
+    nx, ny, nz = dims
+    ic = oracle.ic(dims, 0.05, 0.2, False, 17)
+    want = oracle.run(ic, dims, sp, dt, M, kap, 30, bc)
+    p = mb.make_params(nx, ny, nz, dt, kappa=kap, M=M, dx=sp[0], dy=sp[1], dz=sp[2], bc=bc)
+    with mb.CHSim(p) as sim:
+        assert sim.tiling.path == 0
+        sim.set_field(ic)
+        sim.step(30)
+        got = sim.get_field()
+    assert np.array_equal(got, want), np.abs(got - want).max()
+
+
+def test_fp64_every_tiling_gives_the_same_bits(oracle):
+    dims = (64, 24, 20)
+    ic = oracle.ic(dims, 0.0, 0.2, False, 4)
+    want = oracle.run(ic, dims, (1, 1, 1), 0.005, 1.0, 1.0, 12)
+    p = mb.make_params(*dims, 0.005)
+    seen = 0
+    with mb.CHSim(p) as sim:
+        for ty in (2, 4, 6, 8, 10, 14, 22):
+            for nchunk in (1, 2, 3, 7, 20):
+                for nbuf in (3, 4):
+                    try:
+                        sim.tiling = (ty, nchunk, nbuf, 0)
+                    except mb.MGError:
+                        continue
+                    sim.set_field(ic)
+                    sim.step(12)
+                    got = sim.get_field()
+                    assert np.array_equal(got, want), (ty, nchunk, nbuf)
+                    seen += 1
+    assert seen >= 40
+
+
+def test_graph_replay_equals_single_launches(oracle):
+    dims = (64, 16, 16)
+    ic = oracle.ic(dims, 0.0, 0.2, False, 8)
+    p = mb.make_params(*dims, 0.005)
+    with mb.CHSim(p) as sim:
+        sim.set_field(ic)
+        for _ in range(37):
+            sim.step(1)
+        a = sim.get_field()
+        sim.set_field(ic)
+        sim.step(37)
+        b = sim.get_field()
+        assert sim.steps == 37
+    assert np.array_equal(a, b)
+    assert np.array_equal(a, oracle.run(ic, dims, (1, 1, 1), 0.005, 1.0, 1.0, 37))
+
+
+def test_c1_2d_256_fp64_matches_reference_after_100_steps(oracle):
+    # configuration C1 at 100 steps: 256x256, dt 0.01, U[-0.1, 0.1], seed 42
+    dims = (256, 256, 1)
+    ic = oracle.ic(dims, 0.0, 0.2, False, 42)
+    want = oracle.run(ic, dims, (1, 1, 1), 0.01, 1.0, 1.0, 100)
+    got = run_gpu(mb.make_params(256, 256, 1, 0.01), ic, 100)
+    assert np.array_equal(got, want)
+
+
+def test_c2_3d_128_fp64_matches_oracle(oracle):
+    dims = (128, 128, 128)
+    ic = oracle.ic(dims, 0.0, 0.1, False, 42)
+    want = oracle.run(ic, dims, (1, 1, 1), 0.005, 1.0, 1.0, 10)
+    got = run_gpu(mb.make_params(128, 128, 128, 0.005), ic, 10)
+    assert np.array_equal(got, want)
+
+
+def test_translation_invariance_full_size():
+    # size-independent property at the C2 size: a periodic shift of the input
+    # shifts the output, bit for bit
+    n = 256
+    ic = mb.ic_generate((n, n, n), 0.0, 0.1, False, 42)
+    p = mb.make_params(n, n, n, 0.005)
+    a = run_gpu(p, ic, 20)
+    b = run_gpu(p, np.roll(ic, (37, -11, 5), axis=(0, 1, 2)), 20)
+    assert np.array_equal(b, np.roll(a, (37, -11, 5), axis=(0, 1, 2)))
+
+
+def test_constant_field_fixed_point_and_mass():
+    for prec in ("fp64", "fp32"):
+        p = mb.make_params(64, 32, 16, 0.005, precision=prec)
+        c = np.full((16, 32, 64), 0.3125)
+        assert np.array_equal(run_gpu(p, c, 25), c)
+
+
+def test_fp32_within_tolerance_of_fp64_after_100_steps(oracle):
+    # north-star budget: <= 1e-4 max-norm after 100 steps vs the FP64 oracle
+    dims = (64, 64, 64)
+    ic = oracle.ic(dims, 0.3, 0.02, True, 42)
+    want = oracle.run(ic, dims, (1, 1, 1), 0.005, 1.0, 1.5, 100)
+    for mc in (0, 1):
+        got = run_gpu(mb.make_params(64, 64, 64, 0.005, kappa=1.5, precision="fp32", mass_correct=mc), ic, 100)
+        err = np.abs(got - want).max()
+        assert err <= 1e-4, (mc, err)
+
+
+def test_fp32_mass_feedback_bounds_drift():
+    n = 192
+    ic = mb.ic_generate((n, n, n), 0.3, 0.02, True, 42)
+    p = mb.make_params(n, n, n, 0.005, kappa=1.5, precision="fp32", mass_correct=1)
+    with mb.CHSim(p) as sim:
+        sim.set_field(ic)
+        m0 = sim.reduce()["mass"]
+        for _ in range(4):
+            sim.step(250)
+            r = sim.reduce()
+            assert abs(r["mass"] - m0) / abs(m0) <= 1e-10, r
+
+
+def test_diagnostics_match_oracle(oracle):
+    dims = (64, 40, 24)
+    c = oracle.ic(dims, 0.2, 0.3, False, 6)
+    want = oracle.reduce(c, dims, spacing=(1, 1, 1), kap=1.2)
+    p = mb.make_params(*dims, 0.005, kappa=1.2)
+    with mb.CHSim(p) as sim:
+        sim.set_field(c)
+        got = sim.reduce()
+    for k in ("mass", "energy", "abs_mass"):
+        assert abs(got[k] - want[k]) <= 1e-12 * abs(want[k]), k
+    assert got["max_abs"] == want["max_abs"]
+    assert got["nonfinite"] == 0
+
+
+def test_diagnostics_flag_nonfinite():
+    c = np.zeros((8, 8, 64))
+    c[3, 4, 5] = np.nan
+    c[1, 2, 3] = np.inf
+    with mb.CHSim(mb.make_params(64, 8, 8, 0.005)) as sim:
+        sim.set_field(c)
+        st = sim.reduce(allow_nonfinite=True)
+        assert st["nonfinite"] == 2
+        with pytest.raises(mb.MGError):
+            sim.reduce()
+
+
+def test_structure_factor_matches_numpy(oracle):
+    dims = (64, 32, 16)
+    c = oracle.ic(dims, 0.0, 0.4, False, 2)
+    c = oracle.run(c, dims, (1, 1, 1), 0.01, 1.0, 1.0, 200)
+    kc, sb, cnt, k1 = oracle.structure_factor(c, dims, nbins=40)
+    with mb.CHSim(mb.make_params(*dims, 0.01)) as sim:
+        sim.set_field(c)
+        k, s, g1 = sim.structure_factor(40)
+    assert np.allclose(k, kc, rtol=1e-12, atol=1e-14)
+    assert np.allclose(s, sb, rtol=1e-9, atol=1e-15)
+    assert abs(g1 - k1) <= 1e-9 * k1
+
+
+def test_sync_timeout_then_completion():
+    n = 256
+    with mb.CHSim(mb.make_params(n, n, n, 0.005)) as sim:
+        sim.set_field(mb.ic_generate((n, n, n), 0.0, 0.1, False, 1))
+        sim.step(400)
+        with pytest.raises(mb.MGError) as e:
+            sim.sync(timeout_us=1)
+        assert e.value.code == mb._lib.MG_ETIMEOUT
+        sim.sync()
+        assert sim.steps == 400
+
+
+def test_autotune_picks_a_valid_tiling_with_identical_results(oracle, tmp_path, monkeypatch):
+    monkeypatch.setenv("MG_TUNE_CACHE", str(tmp_path / "tune.json"))
+    p = mb.make_params(64, 32, 32, 0.005)
+    t, ms = mb.autotune(p, trials=3)
+    assert t.path == 0 and ms > 0
+    ic = oracle.ic((64, 32, 32), 0.0, 0.2, False, 3)
+    assert np.array_equal(run_gpu(p, ic, 10, tiling=t), oracle.run(ic, (64, 32, 32), (1, 1, 1), 0.005, 1, 1, 10))
+    assert (tmp_path / "tune.json").exists()

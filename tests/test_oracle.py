@@ -1,0 +1,123 @@
+"""The checker itself: the C restatement (oracle/ch_oracle.c) pinned to the
+golden vectors written by the reference CPU build, to the reference build
+itself when it is present, and to known answers from mathematics."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden_cases, load_golden
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_oracle_matches_reference_golden(oracle, name):
+    meta, arr = load_golden(name)
+    dims = tuple(meta["dims"])
+    ic = oracle.ic(dims, meta["co"], meta["amp"], meta["gaussian"], meta["seed"])
+    assert np.array_equal(ic, arr["ic"]), "seeded initial condition differs from the reference Rand"
+    prev, c = 0, ic
+    for s in meta["steps"]:
+        c = oracle.run(c, dims, meta["spacing"], meta["dt"], meta["M"], meta["kap"], s - prev, meta["bc"])
+        assert np.array_equal(c, arr[f"step{s}"]), f"step {s} differs from the reference build"
+        prev = s
+
+
+def test_mt19937_known_answers(oracle):
+    with open(os.path.join(GOLDEN, "index.json")) as f:
+        idx = json.load(f)
+    for seed, vals in idx["mt19937_first16"].items():
+        assert oracle.mt_u32(int(seed), 16).tolist() == vals
+    # std::mt19937 (default seed 5489): the 10000th output is 4123659995
+    assert int(oracle.mt_u32(5489, 10000)[-1]) == idx["mt19937_5489_10000th"] == 4123659995
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref", "libchref.so")),
+                    reason="reference build not present")
+@pytest.mark.parametrize("case", [
+    ((17, 9, 6), (1.0, 1.0, 1.0), 0.005, 1.0, 1.0, (1, 1, 1)),
+    ((8, 8, 1), (0.75, 1.25, 1.0), 0.001, 2.0, 0.5, (1, 0, 1)),
+    ((6, 5, 4), (1.0, 2.0, 0.5), 0.0005, 0.7, 1.2, (0, 1, 0)),
+    ((1, 9, 7), (1.0, 1.0, 1.0), 0.005, 1.0, 1.0, (1, 1, 1)),
+])
+def test_oracle_matches_reference_build(oracle, case):
+    dims, sp, dt, M, kap, bc = case
+    ic = oracle.ref_ic(dims, 0.05, 0.3, False, 9)
+    a = oracle.ref_run(ic, dims, sp, dt, M, kap, 25, bc)
+    b = oracle.run(ic, dims, sp, dt, M, kap, 25, bc)
+    assert np.array_equal(a, b)
+
+
+def test_constant_field_is_fixed_point(oracle):
+    dims = (7, 5, 3)
+    c = np.full((3, 5, 7), 0.37)
+    out = oracle.run(c, dims, (1, 1, 1), 0.01, 1.0, 1.0, 10)
+    assert np.array_equal(out, c)
+
+
+def test_translation_invariance(oracle):
+    dims = (12, 10, 8)
+    ic = oracle.ic(dims, 0.0, 0.2, False, 5)
+    out = oracle.run(ic, dims, (1, 1, 1), 0.005, 1.0, 1.0, 20)
+    shifted = np.roll(ic, shift=(3, -2, 5), axis=(0, 1, 2))
+    out_s = oracle.run(shifted, dims, (1, 1, 1), 0.005, 1.0, 1.0, 20)
+    assert np.array_equal(out_s, np.roll(out, shift=(3, -2, 5), axis=(0, 1, 2)))
+
+
+def test_linear_growth_rate(oracle):
+    # single Fourier mode of amplitude 1e-8 about c0: amplification per step
+    # 1 + dt*M*lam*(3c0^2 - 1 - kap*lam) to O(eps^2)
+    nx, ny, nz = 16, 8, 4
+    c0, eps, dt, kap = 0.2, 1e-8, 0.01, 1.0
+    x = np.arange(nx)
+    k = 2 * np.pi * 3 / nx
+    c = c0 + eps * np.cos(k * x)[None, None, :] * np.ones((nz, ny, 1))
+    out = oracle.run(c, (nx, ny, nz), (1, 1, 1), dt, 1.0, kap, 1)
+    g = oracle.growth_factor((k, 0, 0), (1, 1, 1), c0, kap, dt)
+    amp = (out - c0)[0, 0, 0] / eps
+    assert abs(amp - g) < 1e-6
+
+
+def test_mass_conserved_and_energy_decays(oracle):
+    dims = (16, 16, 16)
+    c = oracle.ic(dims, 0.1, 0.2, False, 1)
+    r0 = oracle.reduce(c, dims, kap=1.0)
+    prev = r0["energy"]
+    for _ in range(5):
+        c = oracle.run(c, dims, (1, 1, 1), 0.01, 1.0, 1.0, 20)
+        r = oracle.reduce(c, dims, kap=1.0)
+        assert abs(r["mass"] - r0["mass"]) <= 1e-12 * r0["abs_mass"]
+        assert r["energy"] <= prev
+        prev = r["energy"]
+
+
+def test_reduce_compensated_vs_plain(oracle):
+    dims = (64, 32, 16)
+    c = oracle.ic(dims, 0.3, 0.05, True, 42)
+    r = oracle.reduce(c, dims)
+    exact = float(np.sum(c.astype(np.longdouble)))
+    assert abs(r["mass"] - exact) <= abs(r["mass_plain"] - exact) + 1e-9
+    assert abs(r["mass"] - exact) <= 1e-12 * abs(exact)
+
+
+def test_vtk_text_matches_reference_driver(oracle):
+    # golden vtk_ref/ was written by the reference driver (MesoExecute ->
+    # PFApp -> CHBasic -> SfieldFD::writeVTKFile), 8x6x4, iskip 2, 4 steps
+    d = os.path.join(GOLDEN, "vtk_ref")
+    dims = (8, 6, 4)
+    ic = oracle.ic(dims, 0.1, 0.2, False, 5)
+    c2 = oracle.run(ic, dims, (1, 1, 1), 0.01, 1.0, 1.0, 2)
+    c4 = oracle.run(c2, dims, (1, 1, 1), 0.01, 1.0, 1.0, 2)
+    t0 = oracle.vtk_text(ic, dims, "c", 2, 1, 1)
+    assert open(os.path.join(d, "c_0.vtk")).read() == t0 + t0  # written twice at step 0
+    assert open(os.path.join(d, "c_2.vtk")).read() == oracle.vtk_text(c2, dims, "c", 2, 1, 1)
+    assert open(os.path.join(d, "c_4.vtk")).read() == oracle.vtk_text(c4, dims, "c", 2, 1, 1)
+
+
+def test_structure_factor_peak_of_single_mode(oracle):
+    nx = ny = 32
+    k = 2 * np.pi * 4 / nx
+    x = np.arange(nx)
+    c = np.cos(k * x)[None, None, :] * np.ones((1, ny, 1))
+    kc, s, cnt, k1 = oracle.structure_factor(c, (nx, ny, 1))
+    assert abs(k1 - k) < 1e-12
