@@ -60,11 +60,11 @@ def build(verbose: bool = False, force: bool = False) -> str:
         o = os.path.join(BUILD, src + ".o")
         objs.append(o)
         if force or _newer(o, [s] + headers):
-            flags = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+            flags = [NVCC, *ARCH, "-Xptxas=-v", "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
                      f"-I{INCLUDE}", f"-I{CSRC}", "-c", s, "-o", o]
-            if verbose:
-                flags.insert(1, "-Xptxas=-v")
             out = _run(flags, verbose)
+            with open(os.path.join(BUILD, src + ".ptxas.txt"), "w") as f:  # registers / spills per kernel
+                f.write(out)
             if verbose and out:
                 print(out)
     for src in CPP_SOURCES:

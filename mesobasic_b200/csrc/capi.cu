@@ -162,8 +162,8 @@ int mg_autotune(const mg_ch_params* params, int device, int trials, mg_tiling* b
     std::vector<int> tys;
     if (g.flat) tys.push_back(1);
     else
-        for (int ty = 2; ty <= std::min(g.lny, 40); ty += 2) tys.push_back(ty);
-    for (int nbuf = 3; nbuf <= 4; ++nbuf)
+        for (int ty = 1; ty <= std::min(g.lny, 62); ++ty) tys.push_back(ty);
+    for (int nbuf : {3, 4, 6, 8})
         for (int ty : tys) {
             mg_tiling t{ty, 1, nbuf, 0};
             mg::TilePlan pl;
@@ -172,21 +172,23 @@ int mg_autotune(const mg_ch_params* params, int device, int trials, mg_tiling* b
                 continue;
             }
             int occ = 1;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mg::step_kernel(g.es == 4, g.flat, nbuf),
-                                                              pl.block, pl.smem) != cudaSuccess)
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &occ, mg::step_kernel(g.es == 4, g.flat, nbuf, mg::geometry_simple(g), pl.block, g.es == 4, g.lnx), pl.block,
+                    pl.smem) !=
+                cudaSuccess)
                 continue;
             occ = std::max(occ, 1);
             const int slots = h->eng.info.sms * occ;
+            const int maxc = std::max(1, g.lnz / 4);
             std::vector<int> ncs;
             for (int mult = 1; mult <= 3; ++mult) {
-                int nc = std::max(1, mult * slots / pl.ntile);
+                const int nc = std::min(maxc, std::max(1, mult * slots / pl.ntile));
                 ncs.push_back(nc);
                 if (nc > 1) ncs.push_back(nc & ~1);
             }
             std::sort(ncs.begin(), ncs.end());
             ncs.erase(std::unique(ncs.begin(), ncs.end()), ncs.end());
             for (int nc : ncs) {
-                if (nc > g.lnz / 4 && nc > 1) continue;
                 t.nchunk = nc;
                 cands.push_back(t);
             }

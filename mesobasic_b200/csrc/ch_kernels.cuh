@@ -36,21 +36,132 @@
 
 namespace mg {
 
-template <typename T>
-struct alignas(16) Vec {
-    static constexpr int N = 16 / sizeof(T);
-    T v[N];
-};
+// ---------------------------------------------------------------- strips
+// A thread owns a 32-byte strip of one row: 8 floats or 4 doubles.  FP32
+// strips are held as four 64-bit pairs so the arithmetic can use the paired
+// f32x2 instructions of sm_100.
 
 template <typename T>
-__device__ __forceinline__ Vec<T> ld_vec(const T* p)
+struct Strip;
+
+template <>
+struct Strip<float> {
+    static constexpr int W = 8;
+    unsigned long long p[4];
+    __device__ __forceinline__ float get(int e) const
+    {
+        float a, b;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(p[e >> 1]));
+        return (e & 1) ? b : a;
+    }
+};
+
+template <>
+struct Strip<double> {
+    static constexpr int W = 4;
+    double v[4];
+    __device__ __forceinline__ double get(int e) const { return v[e]; }
+};
+
+__device__ __forceinline__ unsigned long long pk2(float a, float b)
 {
-    return *reinterpret_cast<const Vec<T>*>(p);
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
 }
-template <typename T>
-__device__ __forceinline__ void st_vec(T* p, const Vec<T>& q)
+__device__ __forceinline__ float2 upk2(unsigned long long r)
 {
-    *reinterpret_cast<Vec<T>*>(p) = q;
+    float2 a;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+    return a;
+}
+__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c)
+{
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+__device__ __forceinline__ unsigned long long splat2(float a) { return pk2(a, a); }
+
+// A strip is two 16-byte halves: half A at p, half B at p + off (the
+// halves of neighbouring threads are adjacent, so every warp-wide access is
+// one contiguous run and free of bank conflicts).
+template <typename T>
+__device__ __forceinline__ Strip<T> ld_strip(const T* p, int off)
+{
+    Strip<T> s;
+    if constexpr (sizeof(T) == 4) {
+        const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(p);
+        const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(p + off);
+        s.p[0] = a.x, s.p[1] = a.y, s.p[2] = b.x, s.p[3] = b.y;
+    } else {
+        const double2 a = *reinterpret_cast<const double2*>(p);
+        const double2 b = *reinterpret_cast<const double2*>(p + off);
+        s.v[0] = a.x, s.v[1] = a.y, s.v[2] = b.x, s.v[3] = b.y;
+    }
+    return s;
+}
+
+template <typename T>
+__device__ __forceinline__ void st_strip(T* p, int off, const Strip<T>& s)
+{
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<ulonglong2*>(p) = make_ulonglong2(s.p[0], s.p[1]);
+        *reinterpret_cast<ulonglong2*>(p + off) = make_ulonglong2(s.p[2], s.p[3]);
+    } else {
+        *reinterpret_cast<double2*>(p) = make_double2(s.v[0], s.v[1]);
+        *reinterpret_cast<double2*>(p + off) = make_double2(s.v[2], s.v[3]);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void zero_strip(Strip<T>& s)
+{
+    if constexpr (sizeof(T) == 4) {
+        s.p[0] = s.p[1] = s.p[2] = s.p[3] = 0ull;
+    } else {
+        s.v[0] = s.v[1] = s.v[2] = s.v[3] = 0.0;
+    }
+}
+
+// Laplacian numerator sums of a strip with paired FP32 arithmetic, SIMPLE
+// geometry (all periodic, equal spacing): per pair
+// (x sum) + (y sum) + (z sum) - 2*dims*centre.  Half A is pairs 0-1 with x
+// neighbours lA/rA, half B pairs 2-3 with lB/rB.
+template <bool FLAT>
+__device__ __forceinline__ void lap_pairs(const Strip<float>& c, float lA, float rA, float lB, float rB,
+                                          const Strip<float>& up, const Strip<float>& dn, const Strip<float>& zlo,
+                                          const Strip<float>& zhi, unsigned long long (&out)[4])
+{
+    const unsigned long long m6 = splat2(FLAT ? -4.f : -6.f);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int h = k >> 1;  // half
+        const float xm0 = (k & 1) == 0 ? (h == 0 ? lA : lB) : c.get(2 * k - 1);
+        const float xp1 = (k & 1) == 1 ? (h == 0 ? rA : rB) : c.get(2 * k + 2);
+        const unsigned long long sx = pk2(xm0 + c.get(2 * k + 1), c.get(2 * k) + xp1);
+        unsigned long long sacc = add2(sx, add2(zlo.p[k], zhi.p[k]));
+        if constexpr (!FLAT) sacc = add2(sacc, add2(up.p[k], dn.p[k]));
+        out[k] = fma2(c.p[k], m6, sacc);
+    }
 }
 
 // (a[+] + a[-] - 2*a) scaled by c: multiply (power-of-two spacing, exact) or
@@ -61,6 +172,66 @@ __device__ __forceinline__ T axis_term(T plus, T minus, T centre, double c, bool
     using A = Arith<T>;
     T num = A::sub(A::add(plus, minus), A::mul(T(2), centre));
     return divide ? A::div(num, T(c)) : A::mul(num, T(c));
+}
+
+// The 7-point Laplacian of one site in the reference's order
+// ((lapx + lapy) + lapz), SfieldFD.cpp:296-302.  FLAT drops the y term,
+// which is exactly zero in the reference for a flat axis.  SIMPLE (every
+// axis periodic, equal spacing): FP64 skips the multiplications by
+// 1/d^2 = 1, which are exact identities; FP32 uses the algebraically equal
+// ((sum of six neighbours) - 6c) / d^2.
+template <typename T, bool FLAT, bool SIMPLE>
+__device__ __forceinline__ T lap7(T c0, T xp, T xm, T yp, T ym, T zp, T zm, double cx, double cy, double cz,
+                                  bool divX, bool divY, bool divZ)
+{
+    using A = Arith<T>;
+    if constexpr (SIMPLE) {
+        if constexpr (sizeof(T) == 8) {
+            const T c2 = A::mul(T(2), c0);
+            const T lx = A::sub(A::add(xp, xm), c2);
+            const T lz = A::sub(A::add(zp, zm), c2);
+            if constexpr (FLAT) {
+                return A::add(lx, lz);
+            } else {
+                const T ly = A::sub(A::add(yp, ym), c2);
+                return A::add(A::add(lx, ly), lz);
+            }
+        } else {
+            T s = (xp + xm) + (zp + zm);
+            if constexpr (!FLAT) s += (yp + ym);
+            return fmaf(FLAT ? -4.f : -6.f, c0, s) * (float)cx;
+        }
+    } else {
+        if constexpr (FLAT) {
+            return A::add(axis_term(xp, xm, c0, cx, divX), axis_term(zp, zm, c0, cz, divZ));
+        } else {
+            return A::add(A::add(axis_term(xp, xm, c0, cx, divX), axis_term(yp, ym, c0, cy, divY)),
+                          axis_term(zp, zm, c0, cz, divZ));
+        }
+    }
+}
+
+// mu = (c*c*c - c) - kappa*lap (FP64 in that order; FP32 contracted)
+template <typename T>
+__device__ __forceinline__ T chem_pot(T c0, T lap, T kap)
+{
+    if constexpr (sizeof(T) == 8) {
+        using A = Arith<T>;
+        return A::sub(A::sub(A::mul(A::mul(c0, c0), c0), c0), A::mul(kap, lap));
+    } else {
+        return fmaf(-kap, lap, fmaf(c0 * c0, c0, -c0));
+    }
+}
+
+// MurmurHash3's 32-bit finaliser (public domain): a bijective mixer.
+__device__ __forceinline__ uint32_t fmix32(uint32_t h)
+{
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
 }
 
 __device__ __forceinline__ int wrap_or_clamp(int i, int n, bool periodic)
@@ -84,11 +255,30 @@ __device__ __forceinline__ int find_job(const int* item_begin, int njobs, int it
     return lo;
 }
 
-template <typename T, int NBUF, bool FLAT>
-__global__ void __launch_bounds__(512, 1) ch_step_kernel(StepArgs a)
+// Stochastic rounding of s + r onto the FP32 grid: out = RN(s + r + xi*ulp(s))
+// with xi uniform in [-1/2, 1/2), so E[out] = s + r.  Round-to-nearest
+// alone drops every update smaller than half a unit in the last place,
+// and with it the uniform mass correction.
+__device__ __forceinline__ float sr_round(float s, float r, float xi)
 {
-    constexpr int VEC = Vec<T>::N;
-    constexpr int R = FLAT ? 1 : 2;  // rows per thread
+    const float ulp = __uint_as_float(__float_as_uint(s) & 0x7f800000u) * 1.1920928955078125e-7f;
+    return s + fmaf(xi, ulp, r);
+}
+
+// Dither variate in [-1/2, 1/2) from a 32-bit LCG state (top 23 bits).
+__device__ __forceinline__ float lcg_xi(uint32_t& st)
+{
+    st = st * 1664525u + 1013904223u;
+    return __uint_as_float((st >> 9) | 0x3f800000u) - 1.5f;
+}
+
+// NXC: row width fixed at compile time (0: read from the job), so that row,
+// half and piece offsets fold into instruction immediates.
+template <typename T, int NBUF, bool FLAT, bool SIMPLE, bool MASS, int NXC = 0>
+__global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step_kernel(StepArgs a)
+{
+    constexpr int W = Strip<T>::W;  // elements per thread strip
+    constexpr bool PAIRS = (sizeof(T) == 4) && SIMPLE;
     using A = Arith<T>;
 
     extern __shared__ __align__(128) unsigned char smem_dyn[];
@@ -109,7 +299,7 @@ __global__ void __launch_bounds__(512, 1) ch_step_kernel(StepArgs a)
     }
     __syncthreads();
 
-    long long gseq = 0;  // c planes issued by this CTA (ring slot = gseq % NBUF)
+    long long gseq = 0;  // c planes issued by this CTA before the current item
 
     for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
         const int j = find_job(a.item_begin, a.njobs, item);
@@ -122,28 +312,31 @@ __global__ void __launch_bounds__(512, 1) ch_step_kernel(StepArgs a)
         }
         __syncthreads();
         const long long step = head->step;
-        const double delta = head->delta;
+        const float deltaf = (float)head->delta;
         if (step >= J->target) {  // uniform: read once by thread 0
             __syncthreads();        // head->step is rewritten for the next item
             continue;
         }
 
-        const int nx = J->nx, ny = J->ny, nz = J->nz;
-        const int ty = J->ty, flags = J->flags, bw = J->bw;
+        const int nx = NXC ? NXC : J->nx, ny = J->ny, nz = J->nz;
+        const int ty = J->ty, flags = J->flags, bw = NXC ? (NXC < 256 ? NXC : 256) : J->bw;
         const bool perX = flags & JF_PER_X, perY = flags & JF_PER_Y, perZ = flags & JF_PER_Z;
         const bool divX = flags & JF_DIV_X, divY = flags & JF_DIV_Y, divZ = flags & JF_DIV_Z;
-        const bool massfb = flags & JF_MASS;
         const double cx = J->cx, cy = J->cy, cz = J->cz;
         const T kap = T(J->kap), dtM = T(J->dtM);
+        // paired FP32 path: 1/dx^2 folded into kappa and dt*M
+        const float kapc = (float)(J->kap * cx), dtMc = (float)(J->dtM * cx);
+        const uint32_t hkey = fmix32((uint32_t)step * 0x9E3779B9u + 0x632BE5ABu);
         const int par = (int)(step & 1);
         T* __restrict__ dst = static_cast<T*>(J->buf[par ^ 1]);
         const CUtensorMap* tm_body = J->tmap + 2 * par;
         const CUtensorMap* tm_row = J->tmap + 2 * par + 1;
 
         const int CY = FLAT ? 1 : ty + 4;  // c rows in a plane
-        const int MY = FLAT ? 1 : ty + 2;  // mu rows in a plane
+        const int MY = FLAT ? 1 : ty + 2;  // mu rows in a plane (one thread row each)
         const int npiece = nx / bw;
         const uint32_t plane_bytes = (uint32_t)(CY * nx * sizeof(T));
+        const size_t pstride = (size_t)nx * ny;
 
         // ---- tile geometry
         const int tile = local % J->ntile;
@@ -155,47 +348,69 @@ __global__ void __launch_bounds__(512, 1) ch_step_kernel(StepArgs a)
         const int ze = (int)((long long)(chunk + 1) * nz / J->nchunk);
         const int L = ze - zs;
         const int dir = (chunk & 1) ? -1 : 1;
-        auto zseq = [&](int i) { return dir > 0 ? zs - 2 + i : ze + 1 - i; };  // c plane i, i = 0..L+3
+        const int zfirst = dir > 0 ? zs - 2 : ze + 1;  // c plane i lies at z = zfirst + dir*i
+        const int yh0 = FLAT ? 0 : wrap_or_clamp(y0 - 2, ny, perY);
+        const int yh1 = FLAT ? 0 : wrap_or_clamp(y0 - 1, ny, perY);
+        const int yh2 = FLAT ? 0 : wrap_or_clamp(y0 + ty, ny, perY);
+        const int yh3 = FLAT ? 0 : wrap_or_clamp(y0 + ty + 1, ny, perY);
 
-        // ---- thread geometry (fixed for the item)
-        const int nq = nx / VEC;
-        const int ntr = FLAT ? 1 : MY / 2;
-        const int tjob = nq * ntr;
+        // ---- thread geometry (fixed for the item): thread tx of mu row m owns
+        // the 16-byte halves at x = HW*tx (A) and x = HW*tx + nx/2 (B)
+        constexpr int HW = W / 2;
+        const int nq = nx / W;
+        const int tjob = nq * MY;
         const bool active = tid < tjob;
         const int t = active ? tid : 0;
-        const int tx = t % nq, tr = t / nq;
-        const int x0 = tx * VEC;
+        const int tx = t % nq, m = FLAT ? 0 : t / nq;
+        const int xA = tx * HW, xB = xA + nx / 2;
         auto col = [&](int x, int rows) { return (x / bw) * rows * bw + (x % bw); };
-        const int xl = x0 == 0 ? (perX ? nx - 1 : 0) : x0 - 1;
-        const int xr = x0 + VEC >= nx ? (perX ? 0 : nx - 1) : x0 + VEC;
-        const int cOwn = col(x0, CY), cL = col(xl, CY), cR = col(xr, CY);
-        const int mOwn = col(x0, MY), mL = col(xl, MY), mR = col(xr, MY);
-        const bool leftSm = (lane == 0) || (tx == 0);
-        const bool rightSm = (lane == 31) || (tx == nq - 1);
+        auto wrapx = [&](int x) { return x < 0 ? (perX ? x + nx : 0) : (x >= nx ? (perX ? x - nx : nx - 1) : x); };
+        const int cOwn = col(xA, CY), cOffB = col(xB, CY) - cOwn;
+        const int mOwn = col(xA, MY), mOffB = col(xB, MY) - mOwn;
+        // row-relative shared-memory columns of the four x neighbours
+        const int cLA = col(wrapx(xA - 1), CY), cRA = col(xA + HW, CY);
+        const int cLB = col(xB - 1, CY), cRB = col(wrapx(xB + HW), CY);
+        const int mLA = col(wrapx(xA - 1), MY), mRA = col(xA + HW, MY);
+        const int mLB = col(xB - 1, MY), mRB = col(wrapx(xB + HW), MY);
+        // a row of nq threads is a segment of the warp when nq is a power of
+        // two <= 32 (neighbours by lane index, with wrap); otherwise shuffle by
+        // one lane and read the ends of warps and rows from shared memory
+        const bool seg = nq <= 32 && (nq & (nq - 1)) == 0;
+        const int segbase = lane & ~(nq - 1);
+        const int lsrc = seg ? (segbase | ((lane - 1) & (nq - 1))) : ((lane + 31) & 31);
+        const int rsrc = seg ? (segbase | ((lane + 1) & (nq - 1))) : ((lane + 1) & 31);
+        const bool leftSm = !seg && ((lane == 0) || (tx == 0));
+        const bool rightSm = !seg && ((lane == 31) || (tx == nq - 1));
+        const bool first = tx == 0, last = tx == nq - 1;
 
-        // own mu rows m0 = 2*tr, m1 = m0+1 (region row m <-> y = y0 - 1 + m)
-        const int m0 = FLAT ? 0 : 2 * tr;
-        int yrow[2], outrow[2];
-        bool subUp[2], subDn[2];
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const int m = m0 + r;
-            const int y = FLAT ? 0 : y0 - 1 + m;
-            yrow[r] = y;
-            outrow[r] = active && (r < R) && (FLAT || (m >= 1 && m <= ty && y >= own_lo && y < own_hi));
-            subUp[r] = !FLAT && !perY && (y - 1 < 0 || y - 1 >= ny);
-            subDn[r] = !FLAT && !perY && (y + 1 < 0 || y + 1 >= ny);
-        }
+        const int y = FLAT ? 0 : y0 - 1 + m;
+        const size_t rowoff = (size_t)max(y, 0) * nx + xA;
+        const int gOffB = nx / 2;
+        const bool outrow = active && (FLAT || (m >= 1 && m <= ty && y >= own_lo && y < own_hi));
+        const bool subUp = !FLAT && !perY && (y - 1 < 0 || y - 1 >= ny);
+        const bool subDn = !FLAT && !perY && (y + 1 < 0 || y + 1 >= ny);
+        const int cRowOwn = FLAT ? 0 : m + 1;
+        const int mUpRow = FLAT ? 0 : max(m - 1, 0), mDnRow = FLAT ? 0 : min(m + 1, MY - 1);
 
-        auto cplane = [&](long long g) { return cbase + (size_t)(g % NBUF) * a.cplane; };
-        auto mplane = [&](int i) { return mbase + (size_t)(i % 3) * a.mplane; };
+        // c ring: plane i sits in slot (s0 + i) mod NBUF; its barrier phase
+        // flips every time the slot index wraps
+        const int s0 = (int)(gseq % NBUF);
+        const uint32_t ph0 = (uint32_t)((gseq / NBUF) & 1);
+        auto cslot = [&](int i) { return (s0 + i) % NBUF; };
+        auto cphase = [&](int i) { return ph0 ^ (uint32_t)(((s0 + i) / NBUF) & 1); };
+        auto cplane = [&](int i) { return cbase + (size_t)cslot(i) * a.cplane; };
+        auto mplane = [&](int slot) { return mbase + (size_t)slot * a.mplane; };
+        auto zout = [&](int i) { return !perZ && (zfirst + dir * i < 0 || zfirst + dir * i >= nz); };
 
-        // ---- producer: TMA of c plane i into ring slot g
-        auto issue = [&](int i, long long g) {
-            if (tid != 0) return;
-            T* p = cplane(g);
-            uint64_t* bar = &head->bar[g % NBUF];
-            const int zc = wrap_or_clamp(zseq(i), nz, perZ);
+        // ---- producer: TMA of c plane i into its ring slot.  The producer is
+        // the first thread of the last mu row, which has no outputs and so no
+        // stage-B work (thread 0 when flat)
+        const int producer = FLAT ? 0 : (MY - 1) * nq;
+        auto issue = [&](int i) {
+            if (tid != producer) return;
+            T* p = cplane(i);
+            uint64_t* bar = &head->bar[cslot(i)];
+            const int zc = wrap_or_clamp(zfirst + dir * i, nz, perZ);
             mbar_arrive_expect_tx(bar, plane_bytes + a.tx_extra);
             for (int pc = 0; pc < npiece; ++pc) {
                 T* pp = p + (size_t)pc * CY * bw;
@@ -203,190 +418,253 @@ __global__ void __launch_bounds__(512, 1) ch_step_kernel(StepArgs a)
                 if (FLAT) {
                     tma_load_3d(pp, tm_row, bar, xc, 0, zc);
                 } else {
-                    tma_load_3d(pp, tm_row, bar, xc, wrap_or_clamp(y0 - 2, ny, perY), zc);
-                    tma_load_3d(pp + bw, tm_row, bar, xc, wrap_or_clamp(y0 - 1, ny, perY), zc);
+                    tma_load_3d(pp, tm_row, bar, xc, yh0, zc);
+                    tma_load_3d(pp + bw, tm_row, bar, xc, yh1, zc);
                     tma_load_3d(pp + 2 * bw, tm_body, bar, xc, y0, zc);
-                    tma_load_3d(pp + (size_t)(ty + 2) * bw, tm_row, bar, xc, wrap_or_clamp(y0 + ty, ny, perY), zc);
-                    tma_load_3d(pp + (size_t)(ty + 3) * bw, tm_row, bar, xc,
-                                wrap_or_clamp(y0 + ty + 1, ny, perY), zc);
+                    tma_load_3d(pp + (size_t)(ty + 2) * bw, tm_row, bar, xc, yh2, zc);
+                    tma_load_3d(pp + (size_t)(ty + 3) * bw, tm_row, bar, xc, yh3, zc);
                 }
             }
         };
-        auto wait = [&](long long g) {
-            if (!mbar_wait_bounded(&head->bar[g % NBUF], (uint32_t)((g / NBUF) & 1), a.spin_limit)) {
+        auto wait = [&](int i) {
+            if (!mbar_wait_bounded(&head->bar[cslot(i)], cphase(i), a.spin_limit)) {
                 head->abort = 1;
                 atomicMax(&J->err, DEV_TMA_TIMEOUT);
                 atomicMax(a.err, DEV_TMA_TIMEOUT);
             }
         };
-
-        // own values of a c plane: rows m0+1 .. m0+R in c-plane rows
-        auto load_own = [&](const T* p, Vec<T> (&o)[2]) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) o[r] = ld_vec(p + cOwn + (m0 + 1 + r - (FLAT ? 1 : 0)) * bw);
+        // x neighbours of the two halves of a strip: lA/rA left/right of half
+        // A, lB/rB of half B (row-relative shared-memory columns cl*, cr*)
+        auto edges = [&](const Strip<T>& v, const T* rowp, int clA, int crA, int clB, int crB, T& lA, T& rA, T& lB,
+                         T& rB) {
+            const T aF = v.get(0), aL = v.get(HW - 1), bF = v.get(HW), bL = v.get(W - 1);
+            const T sAL = __shfl_sync(0xffffffffu, aL, lsrc), sBL = __shfl_sync(0xffffffffu, bL, lsrc);
+            const T sAF = __shfl_sync(0xffffffffu, aF, rsrc), sBF = __shfl_sync(0xffffffffu, bF, rsrc);
+            if (seg) {
+                // thread 0's left is the last thread's B (A) half; the last
+                // thread's right is thread 0's B (A) half
+                lA = first ? sBL : sAL;
+                lB = first ? sAL : sBL;
+                rA = last ? sBF : sAF;
+                rB = last ? sAF : sBF;
+                if (!perX && first) lA = aF;
+                if (!perX && last) rB = bL;
+            } else {
+                lA = sAL, lB = sBL, rA = sAF, rB = sBF;
+                if (leftSm) {
+                    lA = rowp[clA];
+                    lB = rowp[clB];
+                }
+                if (rightSm) {
+                    rA = rowp[crA];
+                    rB = rowp[crB];
+                }
+            }
         };
 
-        const long long g0 = gseq;
         const int nplanes = L + 4;
         const int npro = min(NBUF, nplanes);
-        for (int i = 0; i < npro; ++i) issue(i, g0 + i);
+        for (int i = 0; i < npro; ++i) issue(i);
         int issued = npro;  // planes issued so far (uniform)
-        int waited = 2;     // planes waited so far (uniform)
-
-        Vec<T> cP[2], cC[2], cN[2], mP[2], mC[2], mN[2];
+        int waited = 0;     // planes waited so far (uniform)
         double macc = 0.0;
 
-        wait(g0);
-        load_own(cplane(g0), cP);
-        wait(g0 + 1);
-        load_own(cplane(g0 + 1), cC);
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-#pragma unroll
-            for (int e = 0; e < VEC; ++e) mP[r].v[e] = mC[r].v[e] = T(0);
-        }
-
-        for (int i = 1; i <= L + 2; ++i) {
-            // c plane i+1 (own values): z neighbour of mu(i)
-            wait(g0 + i + 1);
+        // One plane of the march: mu on plane i (stage A), then c_new on
+        // plane i-1 (stage B).  Register roles rotate between the three call
+        // sites so the z-queue never moves: cp/cc/cn = c(i-1), c(i), c(i+1);
+        // mp/mc/mn = mu(i-2), mu(i-1), mu(i).  mslot/mslot_prev are the mu
+        // ring slots of planes i and i-1 (fixed per call site).
+        auto plane = [&](int i, int mslot, int mslot_prev, Strip<T>& cp, Strip<T>& cc, Strip<T>& cn, Strip<T>& mp,
+                         Strip<T>& mc, Strip<T>& mn) -> bool {
+            wait(i + 1);
             waited = i + 2;
-            load_own(cplane(g0 + i + 1), cN);
-
+            cn = ld_strip(cplane(i + 1) + cOwn + cRowOwn * bw, cOffB);
             // ---- stage A: mu on plane i
             {
-                const T* p = cplane(g0 + i);
-                const int zi = zseq(i);
-                const bool sLo = !perZ && (zseq(i - 1) < 0 || zseq(i - 1) >= nz);
-                const bool sHi = !perZ && (zseq(i + 1) < 0 || zseq(i + 1) >= nz);
-                (void)zi;
-                Vec<T> up, dn;
-                if (!FLAT) {
-                    up = ld_vec(p + cOwn + m0 * bw);
-                    dn = ld_vec(p + cOwn + (m0 + 3) * bw);
+                const T* p = cplane(i);
+                Strip<T> up, dn;
+                if constexpr (!FLAT) {
+                    up = ld_strip(p + cOwn + m * bw, cOffB);
+                    dn = ld_strip(p + cOwn + (m + 2) * bw, cOffB);
                 }
-                T* mp = mplane(i);
+                T lA, rA, lB, rB;
+                const T* rowp = p + cRowOwn * bw;
+                edges(cc, rowp, cLA, cRA, cLB, cRB, lA, rA, lB, rB);
+                if constexpr (PAIRS) {
+                    unsigned long long lp[4];
+                    lap_pairs<FLAT>(cc, lA, rA, lB, rB, up, dn, cp, cn, lp);
+                    const unsigned long long m1 = splat2(-1.f), mk = splat2(-kapc);
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const int crow = FLAT ? 0 : m0 + 1 + r;
-                    T lft = __shfl_up_sync(0xffffffffu, cC[r].v[VEC - 1], 1);
-                    T rgt = __shfl_down_sync(0xffffffffu, cC[r].v[0], 1);
-                    if (leftSm) lft = p[cL + crow * bw];
-                    if (rightSm) rgt = p[cR + crow * bw];
-                    Vec<T> mu;
-#pragma unroll
-                    for (int e = 0; e < VEC; ++e) {
-                        const T c0 = cC[r].v[e];
-                        const T xm = e > 0 ? cC[r].v[e - 1] : lft;
-                        const T xp = e < VEC - 1 ? cC[r].v[e + 1] : rgt;
-                        const T zm = sLo ? c0 : cP[r].v[e];
-                        const T zp = sHi ? c0 : cN[r].v[e];
-                        T lap;
-                        if (FLAT) {
-                            lap = A::add(axis_term(xp, xm, c0, cx, divX), axis_term(zp, zm, c0, cz, divZ));
-                        } else {
-                            T ym = r == 0 ? up.v[e] : cC[0].v[e];
-                            T yp = r == R - 1 ? dn.v[e] : cC[1].v[e];
-                            if (subUp[r]) ym = c0;
-                            if (subDn[r]) yp = c0;
-                            lap = A::add(A::add(axis_term(xp, xm, c0, cx, divX), axis_term(yp, ym, c0, cy, divY)),
-                                         axis_term(zp, zm, c0, cz, divZ));
-                        }
-                        const T df = A::sub(A::mul(A::mul(c0, c0), c0), c0);
-                        mu.v[e] = A::sub(df, A::mul(kap, lap));
+                    for (int k = 0; k < 4; ++k) {
+                        const unsigned long long df = mul2(cc.p[k], fma2(cc.p[k], cc.p[k], m1));
+                        mn.p[k] = fma2(lp[k], mk, df);
                     }
-                    mN[r] = mu;
-                    if (active) st_vec(mp + mOwn + (m0 + r) * bw, mu);
+                } else {
+                    const bool sLo = zout(i - 1), sHi = zout(i + 1);
+                    T mu[W];
+#pragma unroll
+                    for (int e = 0; e < W; ++e) {
+                        const T c0 = cc.get(e);
+                        const int h = e / HW, k = e % HW;
+                        const T xm = k > 0 ? cc.get(e - 1) : (h == 0 ? lA : lB);
+                        const T xp = k < HW - 1 ? cc.get(e + 1) : (h == 0 ? rA : rB);
+                        T zm = cp.get(e), zp = cn.get(e), ym = c0, yp = c0;
+                        if constexpr (!FLAT) {
+                            ym = up.get(e);
+                            yp = dn.get(e);
+                        }
+                        if constexpr (!SIMPLE) {
+                            if (sLo) zm = c0;
+                            if (sHi) zp = c0;
+                            if (subUp) ym = c0;
+                            if (subDn) yp = c0;
+                        }
+                        const T lap = lap7<T, FLAT, SIMPLE>(c0, xp, xm, yp, ym, zp, zm, cx, cy, cz, divX, divY, divZ);
+                        mu[e] = chem_pot(c0, lap, kap);
+                    }
+                    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) mn.p[k] = pk2(mu[2 * k], mu[2 * k + 1]);
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < W; ++e) mn.v[e] = mu[e];
+                    }
                 }
+                if (active) st_strip(mplane(mslot) + mOwn + m * bw, mOffB, mn);
             }
             __syncthreads();
-            if (head->abort) break;
-            // ring slot of plane i-1 is free: refill it with plane i-1+NBUF
-            if (i - 1 + NBUF < nplanes) {
-                issue(i - 1 + NBUF, g0 + i - 1 + NBUF);
-                issued = i + NBUF;
-            }
-
+            if (head->abort) return false;
+            // planes <= i were last read by stage A of this plane (and as `cn`
+            // before it): their ring slots take the planes up to i+NBUF
+            for (; issued <= i + NBUF && issued < nplanes; ++issued) issue(issued);
             // ---- stage B: output plane i-1
             if (i >= 3) {
-                const T* mp = mplane(i - 1);
-                const int zo = zseq(i - 1);
-                const bool sLo = !perZ && (zseq(i - 2) < 0 || zseq(i - 2) >= nz);
-                const bool sHi = !perZ && (zseq(i) < 0 || zseq(i) >= nz);
-                Vec<T> up, dn;
-                if (!FLAT) {
-                    up = ld_vec(mp + mOwn + (m0 > 0 ? m0 - 1 : 0) * bw);
-                    dn = ld_vec(mp + mOwn + (m0 + 2 < MY ? m0 + 2 : MY - 1) * bw);
+                const T* q = mplane(mslot_prev);
+                const int zo = zfirst + dir * (i - 1);
+                const size_t zoff = (size_t)zo * pstride;
+                Strip<T> up, dn;
+                if constexpr (!FLAT) {
+                    up = ld_strip(q + mOwn + mUpRow * bw, mOffB);
+                    dn = ld_strip(q + mOwn + mDnRow * bw, mOffB);
                 }
+                T lA, rA, lB, rB;
+                const int mrow = FLAT ? 0 : m;
+                edges(mc, q + mrow * bw, mLA, mRA, mLB, mRB, lA, rA, lB, rB);
+                if (outrow) {
+                    Strip<T> out;
+                    if constexpr (PAIRS) {
+                        unsigned long long lp[4];
+                        lap_pairs<FLAT>(mc, lA, rA, lB, rB, up, dn, mp, mn, lp);
+                        const unsigned long long dt2 = splat2(dtMc);
+                        if constexpr (MASS) {
+                            uint32_t st = fmix32((uint32_t)((zoff + rowoff) >> 2) + hkey);
+                            const unsigned long long d2 = splat2(deltaf);
+                            unsigned long long acc = 0ull;
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const int mrow = FLAT ? 0 : m0 + r;
-                    T lft = __shfl_up_sync(0xffffffffu, mC[r].v[VEC - 1], 1);
-                    T rgt = __shfl_down_sync(0xffffffffu, mC[r].v[0], 1);
-                    if (leftSm) lft = mp[mL + mrow * bw];
-                    if (rightSm) rgt = mp[mR + mrow * bw];
-                    if (!outrow[r]) continue;
-                    Vec<T> out;
-#pragma unroll
-                    for (int e = 0; e < VEC; ++e) {
-                        const T m = mC[r].v[e];
-                        const T xm = e > 0 ? mC[r].v[e - 1] : lft;
-                        const T xp = e < VEC - 1 ? mC[r].v[e + 1] : rgt;
-                        const T zm = sLo ? m : mP[r].v[e];
-                        const T zp = sHi ? m : mN[r].v[e];
-                        T lap;
-                        if (FLAT) {
-                            lap = A::add(axis_term(xp, xm, m, cx, divX), axis_term(zp, zm, m, cz, divZ));
-                        } else {
-                            T ym = r == 0 ? up.v[e] : mC[0].v[e];
-                            T yp = r == R - 1 ? dn.v[e] : mC[1].v[e];
-                            if (subUp[r]) ym = m;
-                            if (subDn[r]) yp = m;
-                            lap = A::add(A::add(axis_term(xp, xm, m, cx, divX), axis_term(yp, ym, m, cy, divY)),
-                                         axis_term(zp, zm, m, cz, divZ));
-                        }
-                        const T c0 = cP[r].v[e];
-                        T cn;
-                        if constexpr (sizeof(T) == 4) {
-                            if (massfb) {
-                                const T u = lap * dtM;
-                                cn = (T)(((double)c0 + (double)u) + delta);
-                            } else {
-                                cn = fmaf(lap, dtM, c0);
+                            for (int k = 0; k < 4; ++k) {
+                                const unsigned long long u = mul2(lp[k], dt2);
+                                const unsigned long long s2 = add2(cp.p[k], u);
+                                const unsigned long long r2 = add2(sub2(u, sub2(s2, cp.p[k])), d2);
+                                const float2 sv = upk2(s2), rv = upk2(r2);
+                                const float x0v = sr_round(sv.x, rv.x, lcg_xi(st));
+                                const float x1v = sr_round(sv.y, rv.y, lcg_xi(st));
+                                out.p[k] = pk2(x0v, x1v);
+                                acc = k == 0 ? out.p[k] : add2(acc, out.p[k]);
                             }
-                            if (massfb) macc += (double)cn;
+                            const float2 av = upk2(acc);
+                            macc += (double)(av.x + av.y);
                         } else {
-                            cn = A::add(c0, A::mul(lap, dtM));
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) out.p[k] = fma2(lp[k], dt2, cp.p[k]);
                         }
-                        out.v[e] = cn;
+                    } else {
+                        const bool sLo = zout(i - 2), sHi = zout(i);
+                        T o[W];
+                        uint32_t st = 0;
+                        if constexpr (MASS) st = fmix32((uint32_t)((zoff + rowoff) >> 2) + hkey);
+                        float accf = 0.f;
+#pragma unroll
+                        for (int e = 0; e < W; ++e) {
+                            const T mu = mc.get(e);
+                            const int h = e / HW, k = e % HW;
+                            const T xm = k > 0 ? mc.get(e - 1) : (h == 0 ? lA : lB);
+                            const T xp = k < HW - 1 ? mc.get(e + 1) : (h == 0 ? rA : rB);
+                            T zm = mp.get(e), zp = mn.get(e), ym = mu, yp = mu;
+                            if constexpr (!FLAT) {
+                                ym = up.get(e);
+                                yp = dn.get(e);
+                            }
+                            if constexpr (!SIMPLE) {
+                                if (sLo) zm = mu;
+                                if (sHi) zp = mu;
+                                if (subUp) ym = mu;
+                                if (subDn) yp = mu;
+                            }
+                            const T lap = lap7<T, FLAT, SIMPLE>(mu, xp, xm, yp, ym, zp, zm, cx, cy, cz, divX, divY, divZ);
+                            const T c0 = cp.get(e);
+                            if constexpr (sizeof(T) == 4) {
+                                if constexpr (MASS) {
+                                    const float u = lap * dtM;
+                                    const float sv = c0 + u;
+                                    o[e] = sr_round(sv, (u - (sv - c0)) + deltaf, lcg_xi(st));
+                                    accf += o[e];
+                                } else {
+                                    o[e] = fmaf(lap, dtM, c0);
+                                }
+                            } else {
+                                o[e] = A::add(c0, A::mul(lap, dtM));
+                            }
+                        }
+                        if constexpr (sizeof(T) == 4) {
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) out.p[k] = pk2(o[2 * k], o[2 * k + 1]);
+                            if constexpr (MASS) macc += (double)accf;
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < W; ++e) out.v[e] = o[e];
+                        }
                     }
-                    const int y = yrow[r];
-                    st_vec(dst + ((size_t)zo * ny + y) * nx + x0, out);
+                    st_strip(dst + zoff + rowoff, gOffB, out);
                 }
             }
-            // rotate the register planes
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                cP[r] = cC[r];
-                cC[r] = cN[r];
-                mP[r] = mC[r];
-                mC[r] = mN[r];
-            }
-        }
-        gseq = g0 + nplanes;
+            return true;
+        };
 
-        if (head->abort) {
+        Strip<T> c0r, c1r, c2r, m0r, m1r, m2r;
+        zero_strip(m0r);
+        zero_strip(m1r);
+        wait(0);
+        c0r = ld_strip(cplane(0) + cOwn + cRowOwn * bw, cOffB);
+        wait(1);
+        c1r = ld_strip(cplane(1) + cOwn + cRowOwn * bw, cOffB);
+        waited = 2;
+
+        // planes i = 1, 4, 7, ... have i mod 3 == 1: mu slots 1, 2, 0 in turn
+        bool ok = true;
+        int i = 1;
+        for (; ok && i + 2 <= L + 2; i += 3) {
+            ok = plane(i, 1, 0, c0r, c1r, c2r, m0r, m1r, m2r);
+            if (ok) ok = plane(i + 1, 2, 1, c1r, c2r, c0r, m1r, m2r, m0r);
+            if (ok) ok = plane(i + 2, 0, 2, c2r, c0r, c1r, m2r, m0r, m1r);
+        }
+        if (ok && i <= L + 2) {
+            ok = plane(i, 1, 0, c0r, c1r, c2r, m0r, m1r, m2r);
+            ++i;
+        }
+        if (ok && i <= L + 2) ok = plane(i, 2, 1, c1r, c2r, c0r, m1r, m2r, m0r);
+        gseq += nplanes;
+
+        if (!ok) {
             // drain: wait (bounded) for the planes issued but not yet
             // consumed, so no copy lands after the CTA has exited
-            for (int i = waited; i < issued; ++i) {
-                const long long g = g0 + i;
-                mbar_wait_bounded(&head->bar[g % NBUF], (uint32_t)((g / NBUF) & 1), a.spin_limit);
-            }
+            for (int k = waited; k < issued; ++k)
+                mbar_wait_bounded(&head->bar[cslot(k)], cphase(k), a.spin_limit);
             return;
         }
 
         // ---- item epilogue: partial mass, completion count, last-item work
         const int nitems_job = J->ntile * J->nchunk;
-        if (massfb) {
+        if constexpr (MASS) {
             const int nw = (tjob + 31) >> 5;
             double2 v = make_double2(active ? macc : 0.0, 0.0);
 #pragma unroll
@@ -415,7 +693,7 @@ __global__ void __launch_bounds__(512, 1) ch_step_kernel(StepArgs a)
         }
         __syncthreads();
         if (head->flag) {
-            if (massfb && tid < 32) {
+            if (MASS && tid < 32) {
                 double2 r = make_double2(0.0, 0.0);
                 for (int k = lane; k < nitems_job; k += 32) {
                     double2 pv = __ldcg(J->partial + k);
@@ -427,9 +705,9 @@ __global__ void __launch_bounds__(512, 1) ch_step_kernel(StepArgs a)
                     if (lane + off < 32) r = pair_add(r, o);
                 }
                 if (lane == 0) {
-                    const double m = r.x + r.y;
-                    J->mass_last = m;
-                    J->delta = (J->mass_target - m) * J->inv_nsites;
+                    const double mm = r.x + r.y;
+                    J->mass_last = mm;
+                    J->delta = (J->mass_target - mm) * J->inv_nsites;
                 }
             }
             if (tid == 0) {

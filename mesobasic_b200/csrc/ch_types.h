@@ -7,6 +7,13 @@
 
 namespace mg {
 
+// a thread of the step kernel owns 32 bytes of one row: 8 floats or 4 doubles
+constexpr int kStripBytes = 32;
+// largest CTA of the step kernel: 640 threads for the fixed-width variants
+// (at most 102 registers a thread), 512 for the generic one (128 registers)
+constexpr int kMaxBlock = 640;
+constexpr int kMaxBlockGeneric = 512;
+
 enum JobFlags : int {
     JF_PER_X = 1 << 0,
     JF_PER_Y = 1 << 1,
@@ -14,8 +21,9 @@ enum JobFlags : int {
     JF_DIV_X = 1 << 3,  // divide by dx^2 (dx^2 not a power of two), FP64 only
     JF_DIV_Y = 1 << 4,
     JF_DIV_Z = 1 << 5,
-    JF_MASS = 1 << 6,  // FP32 mass-defect feedback
+    JF_MASS = 1 << 6,  // FP32 mass-defect feedback with stochastic rounding
     JF_FLAT = 1 << 7,  // logical ny == 1
+    JF_SIMPLE = 1 << 8,  // all axes periodic, equal spacing (FP64: unit spacing)
 };
 
 enum DeviceError : int {

@@ -4,6 +4,7 @@
 #include "ch_kernels.cuh"
 
 #include <cufft.h>
+#include <dlfcn.h>
 
 #include <algorithm>
 #include <chrono>
@@ -146,17 +147,25 @@ int make_geometry(const mg_ch_params& p, Geometry* out)
 
 bool tma_shape_ok(const Geometry& g)
 {
-    const int vec = 16 / g.es;
-    if (g.lnx % vec != 0) return false;
-    if (g.lnx > 256 && g.lnx % 256 != 0) return false;
+    const int w = kStripBytes / g.es;  // elements per thread strip
+    if (g.lnx % w != 0) return false;
+    // rows wider than one 256-element TMA box: both strip halves (x and
+    // x + nx/2) must sit at the same position of their boxes
+    if (g.lnx > 256 && g.lnx % 512 != 0) return false;
     const int bw = std::min(g.lnx, 256);
     if ((bw * g.es) % 128 != 0) return false;  // 128-byte aligned TMA destinations
-    if (g.flat && g.lnx / vec > 512) return false;
+    if (g.lnx / w > 512) return false;
     if (!g.flat && g.lny < 2) return false;
     return true;
 }
 
 static int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// the step kernel has a compile-time row-width variant for this job
+bool fixed_width_kernel(const Geometry& g, int nbuf)
+{
+    return geometry_simple(g) && !g.flat && (nbuf == 4 || nbuf == 8) && g.lnx == 256;
+}
 
 int plan_tiling(const Geometry& g, const mg_tiling& t, const DevInfo& d, TilePlan* out)
 {
@@ -171,10 +180,9 @@ int plan_tiling(const Geometry& g, const mg_tiling& t, const DevInfo& d, TilePla
     if (t.path != 0) return fail(MG_EINVAL, "tiling path must be 0 or 1");
     if (!tma_shape_ok(g)) return fail(MG_EINVAL, "shape %dx%dx%d (%s) is not taken by the tiled kernel", g.lnx, g.lny,
                                       g.lnz, g.es == 4 ? "fp32" : "fp64");
-    if (t.nbuf != 3 && t.nbuf != 4) return fail(MG_EINVAL, "nbuf must be 3 or 4");
+    if (!nbuf_ok(t.nbuf)) return fail(MG_EINVAL, "nbuf must be 3, 4, 6 or 8");
     if (t.nchunk < 1 || t.nchunk > g.lnz) return fail(MG_EINVAL, "nchunk %d outside [1, %d]", t.nchunk, g.lnz);
-    const int vec = 16 / g.es;
-    const int nq = g.lnx / vec;
+    const int nq = g.lnx / (kStripBytes / g.es);
     int CY, MY, ntr;
     if (g.flat) {
         if (t.ty != 1) return fail(MG_EINVAL, "2-D jobs use ty = 1");
@@ -182,15 +190,16 @@ int plan_tiling(const Geometry& g, const mg_tiling& t, const DevInfo& d, TilePla
         ntr = 1;
         pl.ntile = 1;
     } else {
-        if (t.ty < 2 || t.ty % 2 != 0 || t.ty > g.lny || t.ty > 254)
-            return fail(MG_EINVAL, "ty %d must be even, >= 2 and <= ny (%d)", t.ty, g.lny);
+        if (t.ty < 1 || t.ty > g.lny || t.ty > 252)
+            return fail(MG_EINVAL, "ty %d must be in [1, ny] (ny = %d)", t.ty, g.lny);
         CY = t.ty + 4;
         MY = t.ty + 2;
-        ntr = MY / 2;
+        ntr = MY;  // one mu row per thread row
         pl.ntile = (g.lny + t.ty - 1) / t.ty;
     }
     pl.block = round_up(nq * ntr, 32);
-    if (pl.block > 512) return fail(MG_EINVAL, "tile needs %d threads (> 512); lower ty", nq * ntr);
+    const int maxb = fixed_width_kernel(g, t.nbuf) ? kMaxBlock : kMaxBlockGeneric;
+    if (pl.block > maxb) return fail(MG_EINVAL, "tile needs %d threads (> %d); lower ty", nq * ntr, maxb);
     pl.cplane = round_up(CY * g.lnx, 32);
     pl.mplane = round_up(MY * g.lnx, 32);
     const size_t head = (sizeof(SmemHead) + 127) / 128 * 128 + 128;  // + alignment slack
@@ -203,30 +212,89 @@ int plan_tiling(const Geometry& g, const mg_tiling& t, const DevInfo& d, TilePla
     return MG_OK;
 }
 
-StepKernel step_kernel(bool fp32, bool flat, int nbuf)
+template <typename T, bool FLAT, bool SIMPLE, bool MASS>
+static StepKernel pick_nbuf(int nbuf)
 {
-    if (fp32) {
-        if (flat) return nbuf == 3 ? ch_step_kernel<float, 3, true> : ch_step_kernel<float, 4, true>;
-        return nbuf == 3 ? ch_step_kernel<float, 3, false> : ch_step_kernel<float, 4, false>;
+    switch (nbuf) {
+        case 3: return ch_step_kernel<T, 3, FLAT, SIMPLE, MASS>;
+        case 4: return ch_step_kernel<T, 4, FLAT, SIMPLE, MASS>;
+        case 6: return ch_step_kernel<T, 6, FLAT, SIMPLE, MASS>;
+        default: return ch_step_kernel<T, 8, FLAT, SIMPLE, MASS>;
     }
-    if (flat) return nbuf == 3 ? ch_step_kernel<double, 3, true> : ch_step_kernel<double, 4, true>;
-    return nbuf == 3 ? ch_step_kernel<double, 3, false> : ch_step_kernel<double, 4, false>;
 }
+
+template <typename T, bool FLAT, bool SIMPLE, bool MASS>
+static StepKernel pick_maxt(int nbuf, int /*block*/)
+{
+    return pick_nbuf<T, FLAT, SIMPLE, MASS>(nbuf);
+}
+
+// row widths with a compile-time specialisation of the step kernel
+template <typename T, bool FLAT, bool MASS>
+static StepKernel pick_fixed(int nx, int nbuf)
+{
+    if (nx == 256) return nbuf == 8 ? ch_step_kernel<T, 8, FLAT, true, MASS, 256> : ch_step_kernel<T, 4, FLAT, true, MASS, 256>;
+    return nullptr;
+}
+
+template <typename T, bool MASS>
+static StepKernel pick_shape(bool flat, bool simple, int nbuf, int block)
+{
+    if (flat) return simple ? pick_maxt<T, true, true, MASS>(nbuf, block) : pick_maxt<T, true, false, MASS>(nbuf, block);
+    return simple ? pick_maxt<T, false, true, MASS>(nbuf, block) : pick_maxt<T, false, false, MASS>(nbuf, block);
+}
+
+StepKernel step_kernel(bool fp32, bool flat, int nbuf, bool simple, int block, bool mass, int nx)
+{
+    if (simple && !flat && (nbuf == 4 || nbuf == 8) && nx > 0) {
+        StepKernel k = fp32 ? (mass ? pick_fixed<float, false, true>(nx, nbuf) : pick_fixed<float, false, false>(nx, nbuf))
+                            : pick_fixed<double, false, false>(nx, nbuf);
+        if (k) return k;
+    }
+    if (fp32) return mass ? pick_shape<float, true>(flat, simple, nbuf, block)
+                          : pick_shape<float, false>(flat, simple, nbuf, block);
+    return pick_shape<double, false>(flat, simple, nbuf, block);
+}
+
+bool nbuf_ok(int nbuf) { return nbuf == 3 || nbuf == 4 || nbuf == 6 || nbuf == 8; }
 
 int prepare_kernels(const DevInfo& d)
 {
+    static std::mutex mu;
+    static bool done = false;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done) return MG_OK;
+    const int nbufs[4] = {3, 4, 6, 8};
     for (int f32 = 0; f32 < 2; ++f32)
         for (int fl = 0; fl < 2; ++fl)
-            for (int nb = 3; nb <= 4; ++nb)
-                MG_CUDA(cudaFuncSetAttribute(step_kernel(f32, fl, nb), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)d.smem_optin));
+            for (int sm = 0; sm < 2; ++sm)
+                for (int nb : nbufs)
+                    for (int bl : {256, 512})
+                        for (int ms = 0; ms < 2; ++ms)
+                            for (int fx : {0, 256})
+                            MG_CUDA(cudaFuncSetAttribute(step_kernel(f32, fl, nb, sm, bl, ms && f32, fx),
+                                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                         (int)d.smem_optin));
+    done = true;
     return MG_OK;
+}
+
+// all axes that matter periodic and equal coefficients (FP64: equal to 1,
+// so the multiplication can be skipped exactly)
+bool geometry_simple(const Geometry& g)
+{
+    if (!g.perx || !g.perz || (!g.flat && !g.pery)) return false;
+    const double cx = 1.0 / (g.lsx * g.lsx), cz = 1.0 / (g.lsz * g.lsz), cy = 1.0 / (g.lsy * g.lsy);
+    if (cx != cz || (!g.flat && cx != cy)) return false;
+    if (g.es == 8 && !(g.lsx == 1.0 && g.lsz == 1.0 && (g.flat || g.lsy == 1.0))) return false;
+    return true;
 }
 
 static int occupancy(const Geometry& g, const mg_tiling& t, const TilePlan& pl, int* occ)
 {
-    MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, step_kernel(g.es == 4, g.flat, t.nbuf), pl.block,
-                                                          pl.smem));
+    MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, step_kernel(g.es == 4, g.flat, t.nbuf,
+                                                                      geometry_simple(g), pl.block, g.es == 4, g.lnx),
+                                                          pl.block, pl.smem));
     if (*occ < 1) *occ = 1;
     return MG_OK;
 }
@@ -247,11 +315,11 @@ mg_tiling default_tiling(const Geometry& g, const DevInfo& d, int device)
     // SM, then enough z chunks to fill every CTA slot once, even count so
     // neighbouring chunks march towards / away from each other
     double best_score = -1.0;
-    for (int nbuf = 4; nbuf >= 3; --nbuf) {
+    for (int nbuf : {8, 6, 4, 3}) {
         std::vector<int> tys;
         if (g.flat) tys.push_back(1);
         else
-            for (int ty = 2; ty <= std::min(g.lny, 32); ty += 2) tys.push_back(ty);
+            for (int ty = 1; ty <= std::min(g.lny, 62); ++ty) tys.push_back(ty);
         for (int ty : tys) {
             mg_tiling t{ty, 1, nbuf, 0};
             TilePlan pl;
@@ -275,7 +343,9 @@ mg_tiling default_tiling(const Geometry& g, const DevInfo& d, int device)
             const double rows = g.flat ? 1.0 : (double)ty / (ty + 4);
             const double planes = (double)(g.lnz / nchunk) / (g.lnz / nchunk + 4);
             const double occw = occ >= 2 ? 1.0 : 0.85;
-            const double score = fill * std::sqrt(rows) * planes * occw * (nbuf == 4 ? 1.0 : 0.97);
+            // planes in flight per SM hide the load latency
+            const double inflight = std::min(1.0, (double)(nbuf - 2) * occ * pl.cplane * g.es / (96.0 * 1024));
+            const double score = fill * std::sqrt(rows) * planes * occw * (0.5 + 0.5 * inflight);
             if (score > best_score) {
                 best_score = score;
                 best = mg_tiling{ty, nchunk, nbuf, 0};
@@ -298,12 +368,28 @@ std::string tune_key(const Geometry& g)
     return buf;
 }
 
+// The tuning cache: MG_TUNE_CACHE if set, else tune_cache.json next to
+// this library (measured decompositions shipped with the package).
+static std::string tune_path()
+{
+    const char* env = std::getenv("MG_TUNE_CACHE");
+    if (env) return env;
+    Dl_info info;
+    if (dladdr(reinterpret_cast<void*>(&tune_path), &info) && info.dli_fname) {
+        std::string p = info.dli_fname;
+        const size_t slash = p.rfind('/');
+        return (slash == std::string::npos ? std::string(".") : p.substr(0, slash)) + "/tune_cache.json";
+    }
+    return "";
+}
+
 static void tune_load_file()
 {
     if (g_tune_loaded) return;
     g_tune_loaded = true;
-    const char* path = std::getenv("MG_TUNE_CACHE");
-    if (!path) return;
+    const std::string spath = tune_path();
+    if (spath.empty()) return;
+    const char* path = spath.c_str();
     FILE* f = std::fopen(path, "r");
     if (!f) return;
     std::string s;
@@ -343,7 +429,7 @@ void tune_store(const std::string& key, const mg_tiling& t, double ms)
     std::lock_guard<std::mutex> lock(g_tune_mu);
     tune_load_file();
     g_tune[key] = {t, ms};
-    const char* path = std::getenv("MG_TUNE_CACHE");
+    const char* path = std::getenv("MG_TUNE_CACHE");  // written only where the caller asks
     if (!path) return;
     FILE* f = std::fopen(path, "w");
     if (!f) return;
@@ -385,6 +471,7 @@ static void fill_jobdev(const Job& j, JobDev* jd)
     if (g.perz) flags |= JF_PER_Z;
     if (g.flat) flags |= JF_FLAT;
     if (j.p.mass_correct && g.es == 4) flags |= JF_MASS;
+    if (geometry_simple(g)) flags |= JF_SIMPLE;
     const double sp[3] = {g.lsx, g.lsy, g.lsz};
     double coef[3];
     for (int a = 0; a < 3; ++a) {
@@ -602,10 +689,15 @@ int Engine::rebuild()
             groups_.push_back(g);
             continue;
         }
-        const int key = (j->g.es == 4 ? 1 : 0) | (j->g.flat ? 2 : 0) | (j->tiling.nbuf == 3 ? 4 : 0);
+        const bool simple = geometry_simple(j->g);
+        const bool mass = j->p.mass_correct && j->g.es == 4;
+        const int key = (j->g.es == 4 ? 1 : 0) | (j->g.flat ? 2 : 0) | (simple ? 4 : 0) | (mass ? 8 : 0) |
+                        (j->tiling.nbuf << 4);
         Group& g = by_key[key];
         g.fp32 = j->g.es == 4;
         g.flat = j->g.flat;
+        g.simple = simple;
+        g.mass = mass;
         g.nbuf = j->tiling.nbuf;
         g.jobs.push_back(j);
     }
@@ -624,13 +716,16 @@ int Engine::rebuild()
         }
         begin.push_back(items);
         g.nitems = items;
+        g.fixed_nx = g.jobs.front()->g.lnx;
+        for (Job* j : g.jobs)
+            if (j->g.lnx != g.fixed_nx) g.fixed_nx = 0;
         const int es = g.fp32 ? 4 : 8;
         const size_t head = (sizeof(SmemHead) + 127) / 128 * 128 + 128;  // + alignment slack
         g.smem = head + (size_t)g.nbuf * g.cplane * es + (size_t)3 * g.mplane * es;
         if (g.smem > info.smem_optin) return fail(MG_EINVAL, "batch group needs %zu bytes of shared memory", g.smem);
         int occ = 1;
-        MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_kernel(g.fp32, g.flat, g.nbuf), g.block,
-                                                              g.smem));
+        MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &occ, step_kernel(g.fp32, g.flat, g.nbuf, g.simple, g.block, g.mass, g.fixed_nx), g.block, g.smem));
         occ = std::max(occ, 1);
         g.grid = std::min(items, info.sms * occ);
         MG_CUDA(cudaMalloc(&g.d_item_begin, sizeof(int) * begin.size()));
@@ -684,7 +779,7 @@ int Engine::launch_once()
         a.spin_limit = spin_limit();
         a.err = d_err_;
         a.tx_extra = fault_tx_extra();
-        step_kernel(g.fp32, g.flat, g.nbuf)<<<g.grid, g.block, g.smem, stream>>>(a);
+        step_kernel(g.fp32, g.flat, g.nbuf, g.simple, g.block, g.mass, g.fixed_nx)<<<g.grid, g.block, g.smem, stream>>>(a);
     }
     MG_CUDA(cudaGetLastError());
     return MG_OK;
@@ -890,23 +985,26 @@ int Engine::nlaunch_per_step() const
 
 // ------------------------------------------------------ structure factor
 // Bins |F|^2/N of the half spectrum with Hermitian weights; k = 0 excluded.
-__global__ void sf_bin_kernel(const cufftDoubleComplex* __restrict__ F, int nx, int ny, int nz, double spx,
-                              double spy, double spz, double dk, int nbins, double inv_n, double* __restrict__ acc)
+__global__ void sf_bin_kernel(const cufftDoubleComplex* __restrict__ F, int nx, int ny, int nz, double rx,
+                              double ry, double rz, double dk, int nbins, double inv_n, double* __restrict__ acc)
 {
+    // |k| / dk = sqrt(sum (m_d * L_max / L_d)^2): exact integers on equal
+    // box lengths, so a mode on a bin edge lands in the same bin as in the
+    // host restatement
     const int hx = nx / 2 + 1;
     const size_t total = (size_t)hx * ny * nz;
-    const double two_pi = 6.283185307179586476925286766559;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         const int ix = (int)(i % hx);
         const int iy = (int)((i / hx) % ny);
         const int iz = (int)(i / ((size_t)hx * ny));
         const int fy = iy <= ny / 2 ? iy : iy - ny;
         const int fz = iz <= nz / 2 ? iz : iz - nz;
-        const double kx = two_pi * ix / (nx * spx), ky = two_pi * fy / (ny * spy), kz = two_pi * fz / (nz * spz);
-        const double kk = sqrt(kx * kx + ky * ky + kz * kz);
-        if (kk <= 0.0) continue;
-        const int b = (int)floor(kk / dk);
+        const double qx = ix * rx, qy = fy * ry, qz = fz * rz;
+        const double q = sqrt(qx * qx + qy * qy + qz * qz);
+        if (q <= 0.0) continue;
+        const int b = (int)floor(q + 1e-9);
         if (b >= nbins) continue;
+        const double kk = q * dk;
         const double w = (ix == 0 || (nx % 2 == 0 && ix == nx / 2)) ? 1.0 : 2.0;
         const double s = (F[i].x * F[i].x + F[i].y * F[i].y) * inv_n;
         atomicAdd(acc + 4 * b + 0, w);
@@ -952,8 +1050,8 @@ int Engine::structure_factor(Job* j, int nbins, double* k, double* S, double* k1
         const double L = std::max({nx * p.dx, ny * p.dy, nz * p.dz});
         const double dk = 6.283185307179586476925286766559 / L;
         cudaMemsetAsync(acc, 0, 4 * nbins * sizeof(double), stream);
-        sf_bin_kernel<<<8 * info.sms, 256, 0, stream>>>(F, nx, ny, nz, p.dx, p.dy, p.dz, dk, nbins, 1.0 / (double)n,
-                                                        acc);
+        sf_bin_kernel<<<8 * info.sms, 256, 0, stream>>>(F, nx, ny, nz, L / (nx * p.dx), L / (ny * p.dy),
+                                                        L / (nz * p.dz), dk, nbins, 1.0 / (double)n, acc);
         cudaError_t ce = cudaMemcpyAsync(h.data(), acc, 4 * nbins * sizeof(double), cudaMemcpyDeviceToHost, stream);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(stream);
         if (ce != cudaSuccess) rc = fail(MG_ECUDA, "structure factor: %s", cudaGetErrorString(ce));

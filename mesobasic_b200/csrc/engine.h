@@ -113,10 +113,11 @@ class Engine {
 
    private:
     struct Group {
-        bool fp32 = false, flat = false, generic = false;
+        bool fp32 = false, flat = false, generic = false, simple = false, mass = false;
         int nbuf = 4;
         std::vector<Job*> jobs;
         int nitems = 0, grid = 0, block = 0;
+        int fixed_nx = 0;  // row width shared by every job of the group (0: mixed)
         size_t smem = 0;
         int cplane = 0, mplane = 0;
         int* d_item_begin = nullptr;
@@ -149,7 +150,10 @@ class Engine {
 
 // kernel table
 using StepKernel = void (*)(StepArgs);
-StepKernel step_kernel(bool fp32, bool flat, int nbuf);
+StepKernel step_kernel(bool fp32, bool flat, int nbuf, bool simple, int block, bool mass, int nx = 0);
+bool nbuf_ok(int nbuf);
+bool geometry_simple(const Geometry& g);
+bool fixed_width_kernel(const Geometry& g, int nbuf);
 int prepare_kernels(const DevInfo& d);
 
 }  // namespace mg

@@ -165,14 +165,17 @@ def structure_factor(c, dims, spacing=(1.0, 1.0, 1.0), nbins=None):
     a = np.asarray(c, dtype=np.float64).reshape(nz, ny, nx)
     f = np.fft.fftn(a - a.mean())
     s = (f.real ** 2 + f.imag ** 2) / a.size
-    kx = 2 * np.pi * np.fft.fftfreq(nx, d=spacing[0])
-    ky = 2 * np.pi * np.fft.fftfreq(ny, d=spacing[1])
-    kz = 2 * np.pi * np.fft.fftfreq(nz, d=spacing[2])
-    kk = np.sqrt(kz[:, None, None] ** 2 + ky[None, :, None] ** 2 + kx[None, None, :] ** 2)
-    dk = 2 * np.pi / max(nx * spacing[0], ny * spacing[1], nz * spacing[2])
+    L = max(nx * spacing[0], ny * spacing[1], nz * spacing[2])
+    dk = 2 * np.pi / L
+    # |k|/dk = sqrt(sum (m_d L/L_d)^2), exact integers on equal box lengths
+    mx = np.fft.fftfreq(nx, d=1.0 / nx) * (L / (nx * spacing[0]))
+    my = np.fft.fftfreq(ny, d=1.0 / ny) * (L / (ny * spacing[1]))
+    mz = np.fft.fftfreq(nz, d=1.0 / nz) * (L / (nz * spacing[2]))
+    q = np.sqrt(mz[:, None, None] ** 2 + my[None, :, None] ** 2 + mx[None, None, :] ** 2)
+    kk = q * dk
     if nbins is None:
-        nbins = int(np.floor(kk.max() / dk)) + 1
-    b = np.floor(kk / dk).astype(np.int64)
+        nbins = int(np.floor(q.max() + 1e-9)) + 1
+    b = np.floor(q + 1e-9).astype(np.int64)
     mask = (kk > 0) & (b < nbins)
     sb = np.bincount(b[mask], weights=s[mask], minlength=nbins)
     cnt = np.bincount(b[mask], minlength=nbins)
