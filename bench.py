@@ -63,54 +63,176 @@ def load_traffic(dtype):
 
 
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and throttle reasons sampled through NVML every `period_s`
+    while a timed region runs (start()/stop() around each region; samples
+    accumulate).  Falls back to nvidia-smi when NVML is unavailable."""
 
-    def __init__(self, device):
-        self.device = device
-        self.proc = None
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
-    def __enter__(self):
+    def __init__(self, device, period_s=0.002):
+        self.device, self.period = device, period_s
+        self.sm, self.reasons, self.smax = [], set(), None
+        self._thread, self._stop = None, None
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
-                                         stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
-        return self
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        except Exception:
+            self.nv = None
 
-    def __exit__(self, *exc):
-        self.lines = []
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+    def _sample_nvml(self):
+        nv = self.nv
+        self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+        mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        for name, const in self.REASONS:
+            if mask & getattr(nv, const):
+                self.reasons.add(name)
+
+    def _sample_smi(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        r = subprocess.run(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-i",
+                            str(self.device)], capture_output=True, text=True, timeout=10)
+        parts = [x.strip() for x in r.stdout.strip().split(",")]
+        if len(parts) >= 6:
+            self.sm.append(float(parts[0]))
+            self.smax = float(parts[1])
+            for (name, _), v in zip(self.REASONS, parts[2:6]):
+                if v.lower() == "active":
+                    self.reasons.add(name)
+
+    def start(self):
+        import threading
+        self._stop = threading.Event()
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    self._sample_nvml() if self.nv else self._sample_smi()
+                except Exception:
+                    pass
+                self._stop.wait(self.period if self.nv else 0.2)
+
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
+
+    def stop(self):
+        if self._thread:
+            self._stop.set()
+            self._thread.join()
+            self._thread = None
 
     def summary(self):
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
-            parts = [x.strip() for x in l.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
-            except ValueError:
-                continue
-            for name, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.smax,
+                "reasons": sorted(self.reasons), "samples": len(self.sm),
+                "source": "NVML, every 2 ms inside the timed regions" if self.nv else "nvidia-smi"}
 
 
 # ------------------------------------------------------------------ our arm
+C4_EDGES = (64, 96, 128, 160, 192)
+C5_EDGES_2D = (128, 256, 512, 1024)
+C5_EDGES_3D = (64, 96, 128, 160, 192, 224, 256)
+
+
+def batch_jobs(mb, njobs=64, seed=7):
+    """Batched sweep: njobs cubic grids, edges uniform from C4_EDGES, c0 ~ U[-0.4,0.4],
+    kappa ~ U[0.5,2], uniform noise of amplitude 0.05, per-job IC seed 1000+j."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for j in range(njobs):
+        e = int(rng.choice(C4_EDGES))
+        c0, kap = float(rng.uniform(-0.4, 0.4)), float(rng.uniform(0.5, 2.0))
+        jobs.append(((e, e, e), c0, kap, 1000 + j))
+    return jobs
+
+
+def run_batch(mb, torch, dev, steps, sampler):
+    import numpy as np
+    jobs = batch_jobs(mb)
+    params = [mb.make_params(*d, DT, kappa=k, precision="fp32") for d, _, k, _ in jobs]
+    b = mb.Batch(params, dev)
+    try:
+        for j, (d, c0, _, seed) in enumerate(jobs):
+            b.set_field(j, mb.ic_generate(d, c0, 0.05, False, seed))
+        b.step(3)  # warm-up (and graph capture)
+        b.sync()
+        m0 = [b.reduce(j)["mass"] for j in range(len(jobs))]
+        ext = torch.cuda.ExternalStream(b.stream, device=f"cuda:{dev}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        sampler.start()
+        e0.record(ext)
+        b.step(steps)
+        e1.record(ext)
+        b.sync()
+        torch.cuda.synchronize()
+        sampler.stop()
+        ms = e0.elapsed_time(e1)
+        info = b.info()
+        sites_j = [d[0] * d[1] * d[2] for d, _, _, _ in jobs]
+        # mass drift relative to the mass scale sum|c| ~ N*|c0|+noise: per site
+        drift = max(abs(b.reduce(j)["mass"] - m0[j]) / sites_j[j] for j in range(len(jobs)))
+    finally:
+        b.close()
+    sites = float(sum(d[0] * d[1] * d[2] for d, _, _, _ in jobs))
+    return {"jobs": len(jobs), "sites": sites, "steps": steps, "ms": ms,
+            "value": sites * steps / (ms * 1e-3) / 1e9, "unit": "GLUPS", "precision": "fp32 (mass feedback)",
+            "launches_per_step": info["launches_per_step"], "persistent_ctas": info["ctas"],
+            "max_mass_drift_per_site": drift,
+            "workload": "64 cubic jobs, edges uniform from {64,96,128,160,192}, c0 U[-0.4,0.4], kappa U[0.5,2], "
+                        "noise amplitude 0.05, seeds 1000+j (draws seed 7), dt 0.005",
+            "l2": "fields (about 1.5 GB) larger than L2"}
+
+
+def run_serve(mb, dev, window_s, seed=11, rate=20.0):
+    """Served stream: Poisson arrivals at `rate` jobs/s for `window_s` seconds, then drain."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    arrivals, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > window_s:
+            break
+        if rng.random() < 0.5:
+            e = int(rng.choice(C5_EDGES_2D))
+            dims, dt = (e, e, 1), 0.01
+        else:
+            e = int(rng.choice(C5_EDGES_3D))
+            dims, dt = (e, e, e), DT
+        prec = "fp32" if rng.random() < 0.5 else "fp64"
+        arrivals.append((t, dims, dt, prec, float(rng.uniform(-0.4, 0.4)), float(rng.uniform(0.5, 2.0)),
+                         int(rng.integers(500, 5001)), int(rng.integers(1, 1 << 30))))
+    srv = mb.Server(dev, hbm_budget_gb=150.0, max_jobs=256, steps_per_tick=100)
+    ids = []
+    try:
+        t0 = time.perf_counter()
+        for (ta, dims, dt, prec, c0, kap, nsteps, s) in arrivals:
+            ic = mb.ic_generate(dims, c0, 0.05, False, s)
+            lag = ta - (time.perf_counter() - t0)
+            if lag > 0:
+                time.sleep(lag)
+            p = mb.make_params(*dims, dt, kappa=kap, precision=prec)
+            ids.append((srv.submit(p, ic, nsteps), p))
+        for jid, p in ids:
+            srv.result(jid, p, timeout_us=600_000_000, want_field=False)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+    finally:
+        srv.close()
+    return {"sims_per_hour": st["sims_per_hour"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "mean_ms": st["mean_ms"], "completed": st["completed"], "failed": st["failed"],
+            "glups": st["site_updates_per_s"] / 1e9, "hbm_peak_gb": st["hbm_peak_gb"], "wall_s": wall,
+            "workload": f"Poisson arrivals {rate:g}/s for {window_s:g} s (seed {seed}): 50% 2-D edge "
+                        "{128,256,512,1024} dt 0.01, 50% 3-D edge {64..256 step 32} dt 0.005, 50/50 fp32/fp64, "
+                        "steps U[500,5000], c0 U[-0.4,0.4], kappa U[0.5,2], budget 150 GB, ticks of 100 steps"}
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -126,9 +248,10 @@ def run_ours(args, rank, world, local_rank):
 
     ic = mb.ic_generate((N, N, N), CO, AMP, False, SEED)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+    sampler = ClockSampler(dev)
     results = {}
 
-    def timed_steps(sim, K, W, sampler=None):
+    def timed_steps(sim, K, W):
         ext = torch.cuda.ExternalStream(sim.stream, device=f"cuda:{dev}")
         for _ in range(W):
             sim.step(1)
@@ -137,7 +260,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
-        t0 = time.perf_counter()
+        sampler.start()
         for e0, e1 in evs:
             with torch.cuda.stream(ext):
                 flush.fill_(1)
@@ -146,14 +269,15 @@ def run_ours(args, rank, world, local_rank):
             e1.record(ext)
         sim.sync()
         torch.cuda.synchronize()
+        sampler.stop()
         if dist:
             dist.barrier()
-        wall = time.perf_counter() - t0
         ms = [e0.elapsed_time(e1) for e0, e1 in evs]
-        return sum(ms), ms, wall
+        return sum(ms), ms
 
     def e2e(params, K):
-        """Through the C ABI with pinned host buffers; copies inside the region."""
+        """Through the C ABI with pinned host buffers: upload of the initial
+        field, K steps, download of the final field, all inside the region."""
         host_in = torch.from_numpy(ic.reshape(-1)).pin_memory()
         host_out = torch.empty(N * N * N, dtype=torch.float64).pin_memory()
         with mb.CHSim(params, dev) as sim:
@@ -175,22 +299,27 @@ def run_ours(args, rank, world, local_rank):
         return t
 
     peak, peak_kind = load_peaks()
-    sampler = ClockSampler(dev)
-    with sampler:
-        for prec in ("fp64", "fp32"):
-            params = mb.make_params(N, N, N, DT, kappa=KAP, M=M, precision=prec)
-            with mb.CHSim(params, dev) as sim:
-                sim.set_field(ic)
-                tot_ms, ms, wall = timed_steps(sim, args.steps, args.warmup)
-                tiling = sim.tiling.as_tuple()
-            if dist:
-                tt = torch.tensor([tot_ms], device=f"cuda:{dev}", dtype=torch.float64)
-                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-                tot_ms = float(tt.item())
-            results[prec] = dict(ms_total=tot_ms, ms=ms, wall=wall, tiling=tiling)
-    clocks = sampler.summary()
+    for prec in ("fp64", "fp32"):
+        params = mb.make_params(N, N, N, DT, kappa=KAP, M=M, precision=prec)
+        with mb.CHSim(params, dev) as sim:
+            sim.set_field(ic)
+            tot_ms, ms = timed_steps(sim, args.steps, args.warmup)
+            tiling = sim.tiling.as_tuple()
+        if dist:
+            tt = torch.tensor([tot_ms], device=f"cuda:{dev}", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            tot_ms = float(tt.item())
+        results[prec] = dict(ms_total=tot_ms, ms=ms, tiling=tiling)
     e2e_t = {prec: e2e(mb.make_params(N, N, N, DT, kappa=KAP, M=M, precision=prec), args.steps)
              for prec in ("fp64", "fp32")}
+    batch = run_batch(mb, torch, dev, args.batch_steps, sampler) if args.batch_steps > 0 else None
+    clocks = sampler.summary()
+    serve = run_serve(mb, dev, args.serve_seconds) if args.serve_seconds > 0 else None
+    if batch and dist:
+        tt = torch.tensor([batch["ms"]], device=f"cuda:{dev}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        batch["ms"] = float(tt.item())
+        batch["value"] = world * batch["sites"] * batch["steps"] / (batch["ms"] * 1e-3) / 1e9
 
     if rank != 0:
         if dist:
@@ -212,10 +341,15 @@ def run_ours(args, rank, world, local_rank):
                          "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)",
                          "algorithmic_bytes_per_launch": sites * 2 * es},
             "e2e": {"value": e2e_glups, "unit": "GLUPS", "h2d_bytes_per_step": sites * 8 / args.steps,
-                    "d2h_bytes_per_step": sites * 8 / args.steps},
+                    "d2h_bytes_per_step": sites * 8 / args.steps,
+                    "region": f"upload of the FP64 initial field from pinned memory, {args.steps} steps, download "
+                              "of the final field, through mg_ch_set_field / mg_ch_step / mg_ch_get_field; "
+                              "bytes per step = one field each way / steps"},
             "tiling": {"ty": r["tiling"][0], "nchunk": r["tiling"][1], "nbuf": r["tiling"][2]},
             "ms_per_step_min": min(r["ms"]), "ms_per_step_max": max(r["ms"]),
         }
+    if batch:
+        batch["roofline_frac"] = batch["value"] * 8 / peak  # GB/s of algorithmic bytes / peak
     cpu = cpu_baseline_sample()
     line = {
         "metric": METRIC, "value": out["fp64"]["value"], "unit": "GLUPS", "n_gpus": world,
@@ -228,10 +362,13 @@ def run_ours(args, rank, world, local_rank):
                 | {"dtype": "f32 field, f64 reductions, mass feedback",
                    "speedup_vs_fp64": out["fp32"]["value"] / out["fp64"]["value"]},
         "tiling": out["fp64"]["tiling"],
+        "batch": batch,
+        "serve": serve,
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": args.steps,
-        "gpu_launches_note": "one fused ch_step_kernel launch per timed step (fp64 region); fp32 region likewise",
+        "gpu_launches_note": "one fused ch_step_kernel launch per timed step in the fp64 region (the headline); "
+                             "the fp32 region likewise; the batch region one launch per precision class and step",
     }
     print(json.dumps(line), flush=True)
     if dist:
@@ -279,17 +416,19 @@ def run_reference(args, rank, world):
         return
     cores = host_cores()
     budget_s = 120.0
-    # size the sample: one probe step, then as many steps as fit the budget
-    probe, ranks = run_reference_build(1, cores)
-    per_step = probe["seconds"]
+    # warm-up run (also sizes the sample): W steps, then as many of the K
+    # timed steps as fit the budget
+    probe, ranks = run_reference_build(args.warmup, cores)
+    per_step = probe["seconds"] / max(args.warmup, 1)
     total = args.steps + args.warmup
     steps = max(1, min(args.steps, int(budget_s / max(per_step, 1e-6))))
     d, ranks = run_reference_build(steps, cores)
     glups = d["site_updates_per_s"] / 1e9
     line = {
-        "metric": METRIC, "value": glups, "unit": "GLUPS", "n_gpus": world, "steps": steps, "warmup": 0,
+        "metric": METRIC, "value": glups, "unit": "GLUPS", "n_gpus": world, "steps": steps, "warmup": args.warmup,
         "ms_per_step": d["seconds"] / steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "warmup_note": f"{args.warmup} warm-up steps in a separate run of the same build (it also sizes the sample)",
         "config": dict(CONFIG, precision="fp64", l2="n/a (CPU)"),
         "cpu_baseline": {"value": glups, "unit": "GLUPS", "cores": ranks, "kind": "reference",
                          "sample": f"{steps} of the requested {total} steps of the 256^3 workload on {ranks} "
@@ -305,6 +444,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--batch-steps", type=int, default=1000, help="steps of the batched sweep (0: skip)")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the served stream (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -66,7 +66,7 @@ typedef struct {
 typedef struct {
     int ty;      /* output rows per tile (3-D); 1 for 2-D jobs */
     int nchunk;  /* z chunks (2-D: row chunks) */
-    int nbuf;    /* c planes in flight: 3 or 4 */
+    int nbuf;    /* c planes in the shared-memory ring: 3, 4, 6 or 8 */
     int path;    /* 0 tiled TMA kernel, 1 generic per-site kernel */
 } mg_tiling;
 

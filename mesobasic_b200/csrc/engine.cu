@@ -678,8 +678,33 @@ int Engine::rebuild()
     MG_CUDA(cudaStreamSynchronize(stream));
     drop_graphs();
     free_groups();
-    // one launch per (precision, flat, nbuf) class; generic jobs separately
-    std::map<int, Group> by_key;
+    // Several jobs: one ring depth per class (4 planes for 3-D jobs, 8 for
+    // 2-D) so that each class steps in one launch.  Only nbuf changes; the
+    // tile rows and z chunks, which fix a job's reduction order and so its
+    // results, stay as chosen.
+    if (jobs.size() > 1)
+        for (Job* j : jobs) {
+            if (!j->plan.tma_ok) continue;
+            const int nb = j->g.flat ? 8 : 4;
+            if (j->tiling.nbuf == nb) continue;
+            mg_tiling t = j->tiling;
+            t.nbuf = nb;
+            TilePlan pl;
+            if (plan_tiling(j->g, t, info, &pl) == MG_OK && pl.nitems == j->plan.nitems && pl.ntile == j->plan.ntile) {
+                j->tiling = t;
+                j->plan = pl;
+            } else {
+                clear_error();
+            }
+        }
+    const size_t head = (sizeof(SmemHead) + 127) / 128 * 128 + 128;  // + alignment slack
+    auto group_smem = [&](int nbuf, int cplane, int mplane, int es) {
+        return head + (size_t)nbuf * cplane * es + (size_t)3 * mplane * es;
+    };
+    // one launch per (precision, flat, simple, mass, nbuf, row-width kernel)
+    // class; a class whose planes together outgrow shared memory is split;
+    // generic jobs run on their own
+    std::map<long long, std::vector<Group>> by_key;
     for (Job* j : jobs) {
         if (!j->plan.tma_ok) {
             Group g;
@@ -691,17 +716,31 @@ int Engine::rebuild()
         }
         const bool simple = geometry_simple(j->g);
         const bool mass = j->p.mass_correct && j->g.es == 4;
-        const int key = (j->g.es == 4 ? 1 : 0) | (j->g.flat ? 2 : 0) | (simple ? 4 : 0) | (mass ? 8 : 0) |
-                        (j->tiling.nbuf << 4);
-        Group& g = by_key[key];
+        const int fixed = fixed_width_kernel(j->g, j->tiling.nbuf) ? j->g.lnx : 0;
+        const long long key = (long long)((j->g.es == 4 ? 1 : 0) | (j->g.flat ? 2 : 0) | (simple ? 4 : 0) |
+                                          (mass ? 8 : 0) | (j->tiling.nbuf << 4)) |
+                              ((long long)fixed << 12);
+        std::vector<Group>& gs = by_key[key];
+        const int es = j->g.es;
+        if (gs.empty() || group_smem(j->tiling.nbuf, std::max(gs.back().cplane, j->plan.cplane),
+                                     std::max(gs.back().mplane, j->plan.mplane), es) > info.smem_optin)
+            gs.emplace_back();
+        Group& g = gs.back();
         g.fp32 = j->g.es == 4;
         g.flat = j->g.flat;
         g.simple = simple;
         g.mass = mass;
         g.nbuf = j->tiling.nbuf;
+        g.cplane = std::max(g.cplane, j->plan.cplane);
+        g.mplane = std::max(g.mplane, j->plan.mplane);
         g.jobs.push_back(j);
     }
-    for (auto& kv : by_key) groups_.push_back(kv.second);
+    for (auto& kv : by_key)
+        for (Group& g : kv.second) {
+            g.cplane = 0;
+            g.mplane = 0;
+            groups_.push_back(g);
+        }
     for (Group& g : groups_) {
         if (g.generic) continue;
         std::vector<int> begin, slot;
@@ -719,9 +758,7 @@ int Engine::rebuild()
         g.fixed_nx = g.jobs.front()->g.lnx;
         for (Job* j : g.jobs)
             if (j->g.lnx != g.fixed_nx) g.fixed_nx = 0;
-        const int es = g.fp32 ? 4 : 8;
-        const size_t head = (sizeof(SmemHead) + 127) / 128 * 128 + 128;  // + alignment slack
-        g.smem = head + (size_t)g.nbuf * g.cplane * es + (size_t)3 * g.mplane * es;
+        g.smem = group_smem(g.nbuf, g.cplane, g.mplane, g.fp32 ? 4 : 8);
         if (g.smem > info.smem_optin) return fail(MG_EINVAL, "batch group needs %zu bytes of shared memory", g.smem);
         int occ = 1;
         MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
