@@ -209,6 +209,32 @@ int mg_server_stats_get(mg_server_t* s, mg_server_stats* out);
 /* Stops accepting jobs, finishes the admitted ones, joins the thread. */
 void mg_server_destroy(mg_server_t* s);
 
+/* ----------------------------------------------------------------------
+ * Diagnostics without allocation.  No reference counterpart.
+ * -------------------------------------------------------------------- */
+
+/* The statistics of mg_ch_reduce (mass, |c|, free energy, max|c|,
+ * non-finite count; out->step is set to -1) of a dense x-fastest field
+ * already in device memory on `device` (FP64 or FP32 per params->precision;
+ * nx, ny, nz, spacings, kappa and bx/by/bz are read from params), computed
+ * on `stream` (a cudaStream_t; NULL is the default stream) and waited for at
+ * most timeout_us microseconds (<0: no limit).
+ *
+ * It allocates nothing -- no cudaMalloc/cudaFree, no allocating library
+ * call -- for callers that cannot allocate: a thread that shares the device
+ * with running simulations (an allocation may synchronise the device), a
+ * service whose HBM is fully committed by its admission budget, or code that
+ * holds only a borrowed device pointer and no handle.  Its scratch is one
+ * fixed device array of about 256 KB per process, which bounds the field to
+ * at most 4096 planes (nz for 3-D fields, ny for 2-D ones); larger fields
+ * give MG_EINVAL (use mg_ch_reduce).  The first call on a device looks up
+ * that array's address and should come before any stream capture there.
+ * Calls that overlap in time on one device share the array and race: issue
+ * them one at a time.  Sums are compensated FP64 in a fixed order; they
+ * agree with mg_ch_reduce to rounding (the two sum in different orders). */
+int mg_field_stats_noalloc(const void* field_dev, const mg_ch_params* params, int device, void* stream,
+                           long long timeout_us, mg_ch_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

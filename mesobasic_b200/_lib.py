@@ -105,6 +105,7 @@ SIGNATURES = {
     "mg_server_result": (ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_longlong, _dp, _P(Stats)]),
     "mg_server_stats_get": (ctypes.c_int, [_vp, _P(ServerStats)]),
     "mg_server_destroy": (None, [_vp]),
+    "mg_field_stats_noalloc": (ctypes.c_int, [_vp, _P(Params), ctypes.c_int, _vp, ctypes.c_longlong, _P(Stats)]),
 }
 
 
