@@ -47,10 +47,11 @@ typedef struct {
     int precision;         /* MG_FP64: bit-identical to the reference build;
                               MG_FP32: FP32 field, FP64 reductions */
     int mass_correct;      /* MG_FP32 only: after each step the kernel sums the
-                              stored field in FP64; the next step adds the
-                              uniform correction (target - sum)/N before its
-                              FP32 rounding, so rounding errors of the field do
-                              not accumulate as a drift of total mass */
+                              stored field in FP64, and the next step adds the
+                              defect (target - sum) back as exact nudges of
+                              2^-23 on a window of sites that moves every step,
+                              so rounding errors of the field do not accumulate
+                              as a drift of total mass */
 } mg_ch_params;
 
 typedef struct {

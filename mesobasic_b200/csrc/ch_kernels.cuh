@@ -255,21 +255,20 @@ __device__ __forceinline__ int find_job(const int* item_begin, int njobs, int it
     return lo;
 }
 
-// Stochastic rounding of s + r onto the FP32 grid: out = RN(s + r + xi*ulp(s))
-// with xi uniform in [-1/2, 1/2), so E[out] = s + r.  Round-to-nearest
-// alone drops every update smaller than half a unit in the last place,
-// and with it the uniform mass correction.
-__device__ __forceinline__ float sr_round(float s, float r, float xi)
+// Adds the mass nudge to the elements of a thread's 8-float strip whose sites
+// lie in the nudge window (sites of element e: site0 + e for e < 4, site0 +
+// offB + e - 4 for the second half).  Called only for planes the window
+// reaches, so it stays out of line.
+__device__ __noinline__ void nudge_strip(float* o, long long site0, long long offB, long long w0, long long cnt,
+                                         long long nsites)
 {
-    const float ulp = __uint_as_float(__float_as_uint(s) & 0x7f800000u) * 1.1920928955078125e-7f;
-    return s + fmaf(xi, ulp, r);
-}
-
-// Dither variate in [-1/2, 1/2) from a 32-bit LCG state (top 23 bits).
-__device__ __forceinline__ float lcg_xi(uint32_t& st)
-{
-    st = st * 1664525u + 1013904223u;
-    return __uint_as_float((st >> 9) | 0x3f800000u) - 1.5f;
+    const long long na = cnt < 0 ? -cnt : cnt;
+    const float nudge = cnt < 0 ? -kNudge : kNudge;
+    for (int e = 0; e < 8; ++e) {
+        long long r = site0 + (e < 4 ? e : offB + e - 4) - w0;
+        if (r < 0) r += nsites;
+        if (r < na) o[e] += nudge;
+    }
 }
 
 // NXC: row width fixed at compile time (0: read from the job), so that row,
@@ -295,7 +294,6 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
     if (tid == 0) {
         for (int b = 0; b < NBUF; ++b) mbar_init(&head->bar[b], 1);
         fence_mbar_init();
-        head->abort = 0;
     }
     __syncthreads();
 
@@ -308,11 +306,11 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
 
         if (tid == 0) {
             head->step = *((volatile long long*)&J->step);
-            head->delta = *((volatile double*)&J->delta);
+            head->nudge_begin = *((volatile long long*)&J->nudge_begin);
+            head->nudge_count = *((volatile long long*)&J->nudge_count);
         }
         __syncthreads();
         const long long step = head->step;
-        const float deltaf = (float)head->delta;
         if (step >= J->target) {  // uniform: read once by thread 0
             __syncthreads();        // head->step is rewritten for the next item
             continue;
@@ -326,7 +324,6 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
         const T kap = T(J->kap), dtM = T(J->dtM);
         // paired FP32 path: 1/dx^2 folded into kappa and dt*M
         const float kapc = (float)(J->kap * cx), dtMc = (float)(J->dtM * cx);
-        const uint32_t hkey = fmix32((uint32_t)step * 0x9E3779B9u + 0x632BE5ABu);
         const int par = (int)(step & 1);
         T* __restrict__ dst = static_cast<T*>(J->buf[par ^ 1]);
         const CUtensorMap* tm_body = J->tmap + 2 * par;
@@ -337,6 +334,18 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
         const int npiece = nx / bw;
         const uint32_t plane_bytes = (uint32_t)(CY * nx * sizeof(T));
         const size_t pstride = (size_t)nx * ny;
+        // planes the mass-nudge window reaches: [wz0, wz1], and [0, wz2] for
+        // the part that wraps past the last site
+        int wz0 = 1 << 30, wz1 = -1, wz2 = -1;
+        if constexpr (MASS) {
+            const long long nsites = (long long)pstride * nz, na = llabs(head->nudge_count);
+            if (na > 0) {
+                const long long w0 = head->nudge_begin, w1 = w0 + na;
+                wz0 = (int)(w0 / (long long)pstride);
+                wz1 = (int)((min(w1, nsites) - 1) / (long long)pstride);
+                if (w1 > nsites) wz2 = (int)((w1 - nsites - 1) / (long long)pstride);
+            }
+        }
 
         // ---- tile geometry
         const int tile = local % J->ntile;
@@ -426,9 +435,10 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
                 }
             }
         };
+        bool failed = false;  // a bounded wait of this thread ran out
         auto wait = [&](int i) {
             if (!mbar_wait_bounded(&head->bar[cslot(i)], cphase(i), a.spin_limit)) {
-                head->abort = 1;
+                failed = true;
                 atomicMax(&J->err, DEV_TMA_TIMEOUT);
                 atomicMax(a.err, DEV_TMA_TIMEOUT);
             }
@@ -437,6 +447,15 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
         // A, lB/rB of half B (row-relative shared-memory columns cl*, cr*)
         auto edges = [&](const Strip<T>& v, const T* rowp, int clA, int crA, int clB, int crB, T& lA, T& rA, T& lB,
                          T& rB) {
+            if constexpr (sizeof(T) == 8) {
+                // FP64: from the row in shared memory (a 64-bit value costs two
+                // shuffles and two selects per use)
+                lA = rowp[clA];
+                rA = rowp[crA];
+                lB = rowp[clB];
+                rB = rowp[crB];
+                return;
+            }
             const T aF = v.get(0), aL = v.get(HW - 1), bF = v.get(HW), bL = v.get(W - 1);
             const T sAL = __shfl_sync(0xffffffffu, aL, lsrc), sBL = __shfl_sync(0xffffffffu, bL, lsrc);
             const T sAF = __shfl_sync(0xffffffffu, aF, rsrc), sBF = __shfl_sync(0xffffffffu, bF, rsrc);
@@ -532,8 +551,7 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
                 }
                 if (active) st_strip(mplane(mslot) + mOwn + m * bw, mOffB, mn);
             }
-            __syncthreads();
-            if (head->abort) return false;
+            if (__syncthreads_or(failed)) return false;  // the plane's barrier, and a uniform abort
             // planes <= i were last read by stage A of this plane (and as `cn`
             // before it): their ring slots take the planes up to i+NBUF
             for (; issued <= i + NBUF && issued < nplanes; ++issued) issue(issued);
@@ -550,39 +568,32 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
                 T lA, rA, lB, rB;
                 const int mrow = FLAT ? 0 : m;
                 edges(mc, q + mrow * bw, mLA, mRA, mLB, mRB, lA, rA, lB, rB);
+                // does the mass-nudge window reach into this plane?  (uniform)
+                const bool hit = MASS && ((zo >= wz0 && zo <= wz1) || zo <= wz2);
                 if (outrow) {
                     Strip<T> out;
                     if constexpr (PAIRS) {
                         unsigned long long lp[4];
                         lap_pairs<FLAT>(mc, lA, rA, lB, rB, up, dn, mp, mn, lp);
                         const unsigned long long dt2 = splat2(dtMc);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) out.p[k] = fma2(lp[k], dt2, cp.p[k]);
                         if constexpr (MASS) {
-                            uint32_t st = fmix32((uint32_t)((zoff + rowoff) >> 2) + hkey);
-                            const unsigned long long d2 = splat2(deltaf);
-                            unsigned long long acc = 0ull;
+                            if (hit) {
+                                float o[8];
 #pragma unroll
-                            for (int k = 0; k < 4; ++k) {
-                                const unsigned long long u = mul2(lp[k], dt2);
-                                const unsigned long long s2 = add2(cp.p[k], u);
-                                const unsigned long long r2 = add2(sub2(u, sub2(s2, cp.p[k])), d2);
-                                const float2 sv = upk2(s2), rv = upk2(r2);
-                                const float x0v = sr_round(sv.x, rv.x, lcg_xi(st));
-                                const float x1v = sr_round(sv.y, rv.y, lcg_xi(st));
-                                out.p[k] = pk2(x0v, x1v);
-                                acc = k == 0 ? out.p[k] : add2(acc, out.p[k]);
+                                for (int e = 0; e < 8; ++e) o[e] = out.get(e);
+                                nudge_strip(o, (long long)(zoff + rowoff), gOffB, head->nudge_begin, head->nudge_count,
+                                            (long long)pstride * nz);
+#pragma unroll
+                                for (int k = 0; k < 4; ++k) out.p[k] = pk2(o[2 * k], o[2 * k + 1]);
                             }
-                            const float2 av = upk2(acc);
+                            const float2 av = upk2(add2(add2(out.p[0], out.p[1]), add2(out.p[2], out.p[3])));
                             macc += (double)(av.x + av.y);
-                        } else {
-#pragma unroll
-                            for (int k = 0; k < 4; ++k) out.p[k] = fma2(lp[k], dt2, cp.p[k]);
                         }
                     } else {
                         const bool sLo = zout(i - 2), sHi = zout(i);
                         T o[W];
-                        uint32_t st = 0;
-                        if constexpr (MASS) st = fmix32((uint32_t)((zoff + rowoff) >> 2) + hkey);
-                        float accf = 0.f;
 #pragma unroll
                         for (int e = 0; e < W; ++e) {
                             const T mu = mc.get(e);
@@ -603,22 +614,26 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
                             const T lap = lap7<T, FLAT, SIMPLE>(mu, xp, xm, yp, ym, zp, zm, cx, cy, cz, divX, divY, divZ);
                             const T c0 = cp.get(e);
                             if constexpr (sizeof(T) == 4) {
-                                if constexpr (MASS) {
-                                    const float u = lap * dtM;
-                                    const float sv = c0 + u;
-                                    o[e] = sr_round(sv, (u - (sv - c0)) + deltaf, lcg_xi(st));
-                                    accf += o[e];
-                                } else {
-                                    o[e] = fmaf(lap, dtM, c0);
-                                }
+                                o[e] = fmaf(lap, dtM, c0);
                             } else {
                                 o[e] = A::add(c0, A::mul(lap, dtM));
                             }
                         }
                         if constexpr (sizeof(T) == 4) {
+                            if constexpr (MASS) {
+                                if (hit) {
+                                    float t[8];
+#pragma unroll
+                                    for (int e = 0; e < 8; ++e) t[e] = o[e];
+                                    nudge_strip(t, (long long)(zoff + rowoff), gOffB, head->nudge_begin,
+                                                head->nudge_count, (long long)pstride * nz);
+#pragma unroll
+                                    for (int e = 0; e < 8; ++e) o[e] = t[e];
+                                }
+                                macc += (double)(((o[0] + o[1]) + (o[2] + o[3])) + ((o[4] + o[5]) + (o[6] + o[7])));
+                            }
 #pragma unroll
                             for (int k = 0; k < 4; ++k) out.p[k] = pk2(o[2 * k], o[2 * k + 1]);
-                            if constexpr (MASS) macc += (double)accf;
                         } else {
 #pragma unroll
                             for (int e = 0; e < W; ++e) out.v[e] = o[e];
@@ -707,7 +722,14 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
                 if (lane == 0) {
                     const double mm = r.x + r.y;
                     J->mass_last = mm;
-                    J->delta = (J->mass_target - mm) * J->inv_nsites;
+                    // nudges for the next step; the window moves on by a
+                    // golden-ratio fraction of the field
+                    const long long nsites = (long long)pstride * nz;
+                    double k = rint((J->mass_target - mm) / (double)kNudge);
+                    k = fmin(fmax(k, -(double)nsites), (double)nsites);
+                    J->nudge_count = (long long)k;
+                    const long long stride = (long long)(0.6180339887498949 * (double)nsites) | 1;
+                    J->nudge_begin = (J->nudge_begin + stride) % nsites;
                 }
             }
             if (tid == 0) {
@@ -789,7 +811,8 @@ __global__ void ch_job_reset(JobDev* job, long long target)
         job->target = target;
         job->done = 0;
         job->err = 0;
-        job->delta = 0.0;
+        job->nudge_begin = 0;
+        job->nudge_count = 0;
     }
 }
 
@@ -931,7 +954,8 @@ __global__ void ch_mass_final(const double2* part, int nblocks, JobDev* job)
     if (threadIdx.x == 0) {
         job->mass_target = s.x + s.y;
         job->mass_last = s.x + s.y;
-        job->delta = 0.0;
+        job->nudge_begin = 0;
+        job->nudge_count = 0;
     }
 }
 

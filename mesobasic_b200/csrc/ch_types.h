@@ -21,7 +21,7 @@ enum JobFlags : int {
     JF_DIV_X = 1 << 3,  // divide by dx^2 (dx^2 not a power of two), FP64 only
     JF_DIV_Y = 1 << 4,
     JF_DIV_Z = 1 << 5,
-    JF_MASS = 1 << 6,  // FP32 mass-defect feedback with stochastic rounding
+    JF_MASS = 1 << 6,  // FP32 mass-defect feedback (exact nudges, see kNudge)
     JF_FLAT = 1 << 7,  // logical ny == 1
     JF_SIMPLE = 1 << 8,  // all axes periodic, equal spacing (FP64: unit spacing)
 };
@@ -31,8 +31,17 @@ enum DeviceError : int {
     DEV_TMA_TIMEOUT = 1,  // a TMA completion wait ran out of polls
 };
 
-// Per-job state in device memory.  The host fills the parameters; `delta`,
-// `mass_last`, `step`, `done` and `err` are updated by the kernels.
+// FP32 mass feedback: after each step the kernel sums the stored field in
+// FP64; the defect D = target - sum becomes K = round(D / kNudge) nudges of
+// +-kNudge, which the next step adds to K consecutive sites (a window whose
+// start moves by a fixed stride every step).  kNudge = 2^-23 is a multiple
+// of the unit in the last place of every float below 2 in magnitude, so each
+// nudge is exact there and the stored sum meets the target to within one
+// step's rounding.
+constexpr float kNudge = 1.1920928955078125e-7f;  // 2^-23
+
+// Per-job state in device memory.  The host fills the parameters;
+// `nudge_*`, `mass_last`, `step`, `done` and `err` are updated by the kernels.
 struct alignas(16) JobDev {
     void* buf[2];               // ping-pong fields; step s reads buf[s & 1]
     const CUtensorMap* tmap;    // [2 buffers][body map (bw x ty x 1), row map (bw x 1 x 1)]
@@ -46,7 +55,8 @@ struct alignas(16) JobDev {
     double kap, dtM;            // kappa, dt*M
     double inv_nsites;          // 1 / (nx*ny*nz)
     double mass_target;         // sum(c) of the uploaded field (JF_MASS)
-    double delta;               // uniform correction for the next step (JF_MASS)
+    long long nudge_begin;      // first site of the next step's nudge window (JF_MASS)
+    long long nudge_count;      // sites in the window; the sign is the nudge's
     double mass_last;           // sum(c) after the last step (JF_MASS)
     long long step;             // steps taken
     long long target;           // the job stops stepping here
@@ -73,8 +83,8 @@ struct SmemHead {
     uint64_t bar[8];
     long long step;
     int flag;
-    int abort;
-    double delta;
+    int pad;
+    long long nudge_begin, nudge_count;
     double2 red[32];
 };
 

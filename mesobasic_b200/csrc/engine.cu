@@ -647,7 +647,8 @@ int Engine::set_tiling(Job* j, const mg_tiling& t)
     MG_TRY(read_state(j, h_state_));
     JobDev jd;
     fill_jobdev(*j, &jd);
-    jd.delta = h_state_->delta;
+    jd.nudge_begin = h_state_->nudge_begin;
+    jd.nudge_count = h_state_->nudge_count;
     jd.mass_target = h_state_->mass_target;
     jd.mass_last = h_state_->mass_last;
     jd.step = h_state_->step;
