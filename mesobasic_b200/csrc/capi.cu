@@ -226,6 +226,7 @@ int mg_batch_create(const mg_ch_params* jobs, int njobs, int device, mg_batch_t*
     std::unique_ptr<mg_batch> b(new (std::nothrow) mg_batch);
     if (!b) return fail(MG_ENOMEM, "host allocation failed");
     MG_TRY(b->eng.init(device, njobs));
+    b->eng.batch_tiling = true;
     for (int i = 0; i < njobs; ++i) {
         mg::Job* j = nullptr;
         int rc = b->eng.add_job(jobs[i], -1, &j);

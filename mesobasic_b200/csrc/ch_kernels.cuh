@@ -255,6 +255,17 @@ __device__ __forceinline__ int find_job(const int* item_begin, int njobs, int it
     return lo;
 }
 
+// The stored mass of one thread strip in 2^-32 units: its 8 values summed
+// in FP64 (exact conversions, fixed order), rounded once.  The same function
+// measures the field at upload and after every step.
+__device__ __forceinline__ long long strip_mass(float o0, float o1, float o2, float o3, float o4, float o5, float o6,
+                                                float o7)
+{
+    const double x = ((double)o0 + (double)o2) + ((double)o4 + (double)o6);
+    const double y = ((double)o1 + (double)o3) + ((double)o5 + (double)o7);
+    return __double2ll_rn((x + y) * (double)kMassScale);
+}
+
 // Adds the mass nudge to the elements of a thread's 8-float strip whose sites
 // lie in the nudge window (sites of element e: site0 + e for e < 4, site0 +
 // offB + e - 4 for the second half).  Called only for planes the window
@@ -486,7 +497,7 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
         for (int i = 0; i < npro; ++i) issue(i);
         int issued = npro;  // planes issued so far (uniform)
         int waited = 0;     // planes waited so far (uniform)
-        double macc = 0.0;
+        long long macc = 0;  // stored mass of this thread's strips, 2^-32 units
 
         // One plane of the march: mu on plane i (stage A), then c_new on
         // plane i-1 (stage B).  Register roles rotate between the three call
@@ -588,8 +599,8 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
 #pragma unroll
                                 for (int k = 0; k < 4; ++k) out.p[k] = pk2(o[2 * k], o[2 * k + 1]);
                             }
-                            const float2 av = upk2(add2(add2(out.p[0], out.p[1]), add2(out.p[2], out.p[3])));
-                            macc += (double)(av.x + av.y);
+                            macc += strip_mass(out.get(0), out.get(1), out.get(2), out.get(3), out.get(4), out.get(5),
+                                               out.get(6), out.get(7));
                         }
                     } else {
                         const bool sLo = zout(i - 2), sHi = zout(i);
@@ -630,7 +641,7 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
 #pragma unroll
                                     for (int e = 0; e < 8; ++e) o[e] = t[e];
                                 }
-                                macc += (double)(((o[0] + o[1]) + (o[2] + o[3])) + ((o[4] + o[5]) + (o[6] + o[7])));
+                                macc += strip_mass(o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7]);
                             }
 #pragma unroll
                             for (int k = 0; k < 4; ++k) out.p[k] = pk2(o[2 * k], o[2 * k + 1]);
@@ -680,22 +691,19 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
         // ---- item epilogue: partial mass, completion count, last-item work
         const int nitems_job = J->ntile * J->nchunk;
         if constexpr (MASS) {
+            // |strip| < 2^36 units, a thread holds at most nz strips, a CTA
+            // at most 640 threads: the item sum fits 64 bits
+            long long* red = reinterpret_cast<long long*>(head->red);
             const int nw = (tjob + 31) >> 5;
-            double2 v = make_double2(active ? macc : 0.0, 0.0);
+            long long v = active ? macc : 0;
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                double2 o = shfl_down_pair(v, off);
-                if (lane + off < 32) v = pair_add(v, o);
-            }
-            if (lane == 0 && (tid >> 5) < nw) head->red[tid >> 5] = v;
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0 && (tid >> 5) < nw) red[tid >> 5] = v;
             __syncthreads();
             if (tid < 32) {
-                double2 r = lane < nw ? head->red[lane] : make_double2(0.0, 0.0);
+                long long r = lane < nw ? red[lane] : 0;
 #pragma unroll
-                for (int off = 16; off > 0; off >>= 1) {
-                    double2 o = shfl_down_pair(r, off);
-                    if (lane + off < 32) r = pair_add(r, o);
-                }
+                for (int off = 16; off > 0; off >>= 1) r += __shfl_down_sync(0xffffffffu, r, off);
                 if (lane == 0) J->partial[local] = r;
             }
         }
@@ -709,18 +717,16 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
         __syncthreads();
         if (head->flag) {
             if (MASS && tid < 32) {
-                double2 r = make_double2(0.0, 0.0);
-                for (int k = lane; k < nitems_job; k += 32) {
-                    double2 pv = __ldcg(J->partial + k);
-                    r = pair_add(r, pv);
-                }
+                __int128 r = 0;
+                for (int k = lane; k < nitems_job; k += 32) r += __ldcg(J->partial + k);
 #pragma unroll
                 for (int off = 16; off > 0; off >>= 1) {
-                    double2 o = shfl_down_pair(r, off);
-                    if (lane + off < 32) r = pair_add(r, o);
+                    const unsigned long long lo = __shfl_down_sync(0xffffffffu, (unsigned long long)r, off);
+                    const long long hi = __shfl_down_sync(0xffffffffu, (long long)(r >> 64), off);
+                    r += ((__int128)hi << 64) | (__int128)lo;
                 }
                 if (lane == 0) {
-                    const double mm = r.x + r.y;
+                    const double mm = (double)r / (double)kMassScale;
                     J->mass_last = mm;
                     // nudges for the next step; the window moves on by a
                     // golden-ratio fraction of the field
@@ -930,33 +936,43 @@ __global__ void ch_diag_final(const double2* part, const double* pmax, const dou
     }
 }
 
-// Sum of the stored field (no dV), for the FP32 mass target.
-template <typename T>
-__global__ void ch_mass_partial(const JobDev* job, double2* part)
+// Stored mass of an uploaded FP32 field, measured as the step kernel
+// measures it (strip_mass, 2^-32 units): the FP32 mass target.
+__global__ void ch_mass_partial(const JobDev* job, long long* part)
 {
-    __shared__ double2 scratch[32];
+    __shared__ long long red[32];
     const JobDev& J = *job;
-    const size_t n = (size_t)J.nx * J.ny * J.nz;
-    const T* c = static_cast<const T*>(J.buf[J.step & 1]);
-    double2 s = make_double2(0, 0);
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        s = pair_add(s, make_double2((double)c[i], 0.0));
-    s = block_pair_sum(s, scratch);
-    if (threadIdx.x == 0) part[blockIdx.x] = s;
+    const int nx = J.nx, nq = nx / 8;
+    const long long nstrips = (long long)J.ny * J.nz * nq;
+    const float* c = static_cast<const float*>(J.buf[J.step & 1]);
+    long long s = 0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nstrips;
+         t += (long long)gridDim.x * blockDim.x) {
+        const float* row = c + (t / nq) * nx;
+        const int xa = 4 * (int)(t % nq), xb = xa + nx / 2;
+        s += strip_mass(row[xa], row[xa + 1], row[xa + 2], row[xa + 3], row[xb], row[xb + 1], row[xb + 2], row[xb + 3]);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long b = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += red[w];
+        part[blockIdx.x] = b;
+    }
 }
 
-__global__ void ch_mass_final(const double2* part, int nblocks, JobDev* job)
+__global__ void ch_mass_final(const long long* part, int nblocks, JobDev* job)
 {
-    __shared__ double2 scratch[32];
-    double2 s = make_double2(0, 0);
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s = pair_add(s, part[b]);
-    s = block_pair_sum(s, scratch);
-    if (threadIdx.x == 0) {
-        job->mass_target = s.x + s.y;
-        job->mass_last = s.x + s.y;
-        job->nudge_begin = 0;
-        job->nudge_count = 0;
-    }
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __int128 s = 0;
+    for (int b = 0; b < nblocks; ++b) s += part[b];
+    const double m = (double)s / (double)kMassScale;
+    job->mass_target = m;
+    job->mass_last = m;
+    job->nudge_begin = 0;
+    job->nudge_count = 0;
 }
 
 }  // namespace mg

@@ -40,12 +40,19 @@ enum DeviceError : int {
 // step's rounding.
 constexpr float kNudge = 1.1920928955078125e-7f;  // 2^-23
 
+// The stored mass is measured the same way by the step kernel and at upload,
+// independent of the decomposition: each thread strip's 8 values are summed
+// in FP64 in one fixed order (strip_mass), the sum is rounded to a multiple
+// of 2^-32 and the integers are added (integer addition does not depend on
+// order).  A strip is the 8 sites x = 4t..4t+3 and nx/2 + 4t..4t+3 of a row.
+constexpr float kMassScale = 4294967296.0f;  // 2^32
+
 // Per-job state in device memory.  The host fills the parameters;
 // `nudge_*`, `mass_last`, `step`, `done` and `err` are updated by the kernels.
 struct alignas(16) JobDev {
     void* buf[2];               // ping-pong fields; step s reads buf[s & 1]
     const CUtensorMap* tmap;    // [2 buffers][body map (bw x ty x 1), row map (bw x 1 x 1)]
-    double2* partial;           // per-item mass pairs (JF_MASS)
+    long long* partial;         // per-item stored-mass sums in 2^-32 units (JF_MASS)
     int nx, ny, nz;             // logical dims (2-D jobs: nx, 1, ny)
     int ty;                     // output rows per tile (1 when flat)
     int ntile, nchunk;          // y tiles x z chunks = items

@@ -355,6 +355,37 @@ mg_tiling default_tiling(const Geometry& g, const DevInfo& d, int device)
     return best;
 }
 
+// Tiling of a job that shares its launches with other jobs (batch, server).
+// Every job gets tiles of about kBatchThreads threads (ty + 2 mu rows of
+// nx/W strips), so the CTAs of one launch are equally full whatever each
+// job's row width; tiles are balanced to divide ny evenly; z chunks are about
+// 64 planes (many jobs fill the grid, so no job is cut finer).  A pure
+// function of the shape: a job keeps its tiling for its whole life.
+mg_tiling batch_tiling_for(const Geometry& g, const DevInfo& d, int device)
+{
+    if (!tma_shape_ok(g)) return default_tiling(g, d, device);
+    constexpr int kBatchThreads = 256;
+    const int nq = g.lnx / (kStripBytes / g.es);
+    const int nbuf = g.flat ? 8 : 4;
+    int ty = 1;
+    if (!g.flat) {
+        const int maxb = fixed_width_kernel(g, nbuf) ? kMaxBlock : kMaxBlockGeneric;
+        int tymax = std::max(1, kBatchThreads / nq - 2);
+        tymax = std::max(tymax, std::min(8, std::max(1, maxb / nq - 2)));  // at least 8 rows where they fit
+        tymax = std::min(tymax, g.lny);
+        const int ntile = (g.lny + tymax - 1) / tymax;
+        ty = (g.lny + ntile - 1) / ntile;
+    }
+    mg_tiling t{ty, std::max(1, g.lnz / 64), nbuf, 0};
+    TilePlan pl;
+    while (plan_tiling(g, t, d, &pl) != MG_OK) {  // shrink the tile until it fits
+        clear_error();
+        if (t.ty <= 1) return default_tiling(g, d, device);
+        t.ty -= 1;
+    }
+    return t;
+}
+
 // ------------------------------------------------------------ autotune cache
 static std::mutex g_tune_mu;
 static std::map<std::string, std::pair<mg_tiling, double>> g_tune;
@@ -447,7 +478,7 @@ void tune_store(const std::string& key, const mg_tiling& t, double ms)
 // ------------------------------------------------------------------ Job
 size_t Job::device_bytes() const
 {
-    return 2 * g.n * g.es + 4 * sizeof(CUtensorMap) + (size_t)std::max(plan.nitems, 1) * sizeof(double2);
+    return 2 * g.n * g.es + 4 * sizeof(CUtensorMap) + (size_t)std::max(plan.nitems, 1) * sizeof(long long);
 }
 
 static void fill_jobdev(const Job& j, JobDev* jd)
@@ -550,7 +581,7 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out)
     MG_TRY(make_geometry(p, &j->g));
     if (free_slots_.empty()) return fail(MG_ENOMEM, "no free job slot (capacity %d)", capacity_);
     MG_CUDA(cudaSetDevice(device));
-    j->tiling = default_tiling(j->g, info, device);
+    j->tiling = batch_tiling ? batch_tiling_for(j->g, info, device) : default_tiling(j->g, info, device);
     MG_TRY(plan_tiling(j->g, j->tiling, info, &j->plan));
     if (j->p.mass_correct && !j->plan.tma_ok)
         return fail(MG_EINVAL, "mass_correct needs a shape the tiled kernel takes (nx multiple of %d)", 32);
@@ -559,7 +590,7 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out)
     cudaError_t e = cudaMalloc(&j->buf[0], bytes);
     if (e == cudaSuccess) e = cudaMalloc(&j->buf[1], bytes);
     if (e == cudaSuccess) e = cudaMalloc(&j->d_tmap, 4 * sizeof(CUtensorMap));
-    if (e == cudaSuccess) e = cudaMalloc(&j->d_partial, sizeof(double2) * std::max(j->plan.nitems, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&j->d_partial, sizeof(long long) * std::max(j->plan.nitems, 1));
     if (e != cudaSuccess) {
         cudaGetLastError();
         cudaFree(j->buf[0]);
@@ -615,8 +646,8 @@ int Engine::set_tiling(Job* j, const mg_tiling& t)
     MG_TRY(plan_tiling(j->g, t, info, &pl));
     if (j->p.mass_correct && !pl.tma_ok) return fail(MG_EINVAL, "mass_correct needs the tiled kernel");
     MG_CUDA(cudaStreamSynchronize(stream));
-    double2* part = nullptr;
-    MG_CUDA(cudaMalloc(&part, sizeof(double2) * std::max(pl.nitems, 1)));
+    long long* part = nullptr;
+    MG_CUDA(cudaMalloc(&part, sizeof(long long) * std::max(pl.nitems, 1)));
     const mg_tiling old = j->tiling;
     const TilePlan old_plan = j->plan;
     j->tiling = t;
@@ -939,8 +970,10 @@ int Engine::upload(Job* j, const double* host, long long target)
     j->target = target;
     ch_job_reset<<<1, 32, 0, stream>>>(d_jobs_ + j->slot, target < 0 ? LLONG_MAX : target);
     if (j->g.es == 4) {
-        ch_mass_partial<float><<<kDiagBlocks, kDiagThreads, 0, stream>>>(d_jobs_ + j->slot, d_diag_part_);
-        ch_mass_final<<<1, 256, 0, stream>>>(d_diag_part_, kDiagBlocks, d_jobs_ + j->slot);
+        // d_diag_part_ (3 x kDiagBlocks double2) is scratch for the block sums
+        long long* part = reinterpret_cast<long long*>(d_diag_part_);
+        ch_mass_partial<<<kDiagBlocks, kDiagThreads, 0, stream>>>(d_jobs_ + j->slot, part);
+        ch_mass_final<<<1, 32, 0, stream>>>(part, kDiagBlocks, d_jobs_ + j->slot);
     }
     MG_CUDA(cudaGetLastError());
     return MG_OK;

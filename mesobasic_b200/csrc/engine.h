@@ -77,7 +77,7 @@ struct Job {
     TilePlan plan;
     void* buf[2] = {nullptr, nullptr};
     CUtensorMap* d_tmap = nullptr;  // 4 maps
-    double2* d_partial = nullptr;
+    long long* d_partial = nullptr;
     int slot = -1;
     long long target = -1;  // device step target (-1: unbounded)
     size_t device_bytes() const;
@@ -107,6 +107,9 @@ class Engine {
     int nlaunch_per_step() const;
 
     int device = 0;
+    // jobs share launches (batch, server): tile every job for equally full
+    // CTAs (batch_tiling_for) instead of for the fastest standalone run
+    bool batch_tiling = false;
     cudaStream_t stream = nullptr;
     DevInfo info;
     std::vector<Job*> jobs;
