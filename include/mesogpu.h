@@ -189,6 +189,12 @@ typedef struct {
     double sims_per_hour;        /* completed / wall time since the first arrival */
     double site_updates_per_s;   /* sum(sites*steps) of completed jobs / wall time */
     double hbm_in_use_gb, hbm_peak_gb;
+    /* where the worker thread's time went: enqueueing and waiting for step
+       ticks (GPU busy), admitting jobs (allocation, upload), retiring jobs
+       (download, diagnostics); ticks run and launch-set rebuilds (each
+       recaptures the step graph) */
+    double step_s, admit_s, retire_s;
+    long long ticks, rebuilds;
 } mg_server_stats;
 
 #define MG_JOB_QUEUED 0

@@ -59,7 +59,9 @@ class ServerStats(ctypes.Structure):
                 ("failed", ctypes.c_longlong), ("running", ctypes.c_longlong), ("queued", ctypes.c_longlong),
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
                 ("sims_per_hour", ctypes.c_double), ("site_updates_per_s", ctypes.c_double),
-                ("hbm_in_use_gb", ctypes.c_double), ("hbm_peak_gb", ctypes.c_double)]
+                ("hbm_in_use_gb", ctypes.c_double), ("hbm_peak_gb", ctypes.c_double),
+                ("step_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("retire_s", ctypes.c_double),
+                ("ticks", ctypes.c_longlong), ("rebuilds", ctypes.c_longlong)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -359,7 +359,8 @@ mg_tiling default_tiling(const Geometry& g, const DevInfo& d, int device)
 // Every job gets tiles of about kBatchThreads threads (ty + 2 mu rows of
 // nx/W strips), so the CTAs of one launch are equally full whatever each
 // job's row width; tiles are balanced to divide ny evenly; z chunks are about
-// 64 planes (many jobs fill the grid, so no job is cut finer).  A pure
+// 64 planes (16 rows for 2-D jobs; many jobs fill the grid, so no job is cut
+// finer).  A pure
 // function of the shape: a job keeps its tiling for its whole life.
 mg_tiling batch_tiling_for(const Geometry& g, const DevInfo& d, int device)
 {
@@ -376,7 +377,9 @@ mg_tiling batch_tiling_for(const Geometry& g, const DevInfo& d, int device)
         const int ntile = (g.lny + tymax - 1) / tymax;
         ty = (g.lny + ntile - 1) / ntile;
     }
-    mg_tiling t{ty, std::max(1, g.lnz / 64), nbuf, 0};
+    // 2-D jobs march along their rows one row per plane: shorter chunks give
+    // them enough CTAs
+    mg_tiling t{ty, std::max(1, g.lnz / (g.flat ? 16 : 64)), nbuf, 0};
     TilePlan pl;
     while (plan_tiling(g, t, d, &pl) != MG_OK) {  // shrink the tile until it fits
         clear_error();
@@ -549,6 +552,10 @@ Engine::~Engine()
     cudaFree(d_diag_);
     cudaFreeHost(h_diag_);
     cudaFreeHost(h_state_);
+    free_graveyard();
+    for (cudaStream_t st : aux_) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : aux_ev_) cudaEventDestroy(ev);
+    if (fork_ev_) cudaEventDestroy(fork_ev_);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -631,10 +638,9 @@ void Engine::remove_job(Job* j)
     auto it = std::find(jobs.begin(), jobs.end(), j);
     if (it == jobs.end()) return;
     jobs.erase(it);
-    cudaFree(j->buf[0]);
-    cudaFree(j->buf[1]);
-    cudaFree(j->d_tmap);
-    cudaFree(j->d_partial);
+    // freed at the next rebuild (which waits for the stream anyway) or at
+    // destruction: cudaFree waits for the whole device, once per call
+    graveyard_.insert(graveyard_.end(), {j->buf[0], j->buf[1], (void*)j->d_tmap, (void*)j->d_partial});
     free_slots_.push_back(j->slot);
     delete j;
     dirty_ = true;
@@ -705,9 +711,17 @@ void Engine::drop_graphs()
     graphs_.clear();
 }
 
+void Engine::free_graveyard()
+{
+    for (void* p : graveyard_) cudaFree(p);
+    graveyard_.clear();
+}
+
 int Engine::rebuild()
 {
+    ++rebuilds_;
     MG_CUDA(cudaStreamSynchronize(stream));
+    free_graveyard();
     drop_graphs();
     free_groups();
     // Several jobs: one ring depth per class (4 planes for 3-D jobs, 8 for
@@ -802,6 +816,21 @@ int Engine::rebuild()
         MG_CUDA(cudaMemcpy(g.d_item_begin, begin.data(), sizeof(int) * begin.size(), cudaMemcpyHostToDevice));
         MG_CUDA(cudaMemcpy(g.d_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice));
     }
+    // streams and events of the lanes (created here, never inside a capture)
+    size_t lanes = 0;
+    for (const Group& g : groups_) lanes += g.generic ? g.jobs.size() : 1;
+    while (lanes > 1 && aux_.size() < lanes) {
+        cudaStream_t st;
+        cudaEvent_t ev;
+        MG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaStreamDestroy(st);
+            return fail(MG_ECUDA, "creating a lane event failed");
+        }
+        aux_.push_back(st);
+        aux_ev_.push_back(ev);
+    }
+    if (lanes > 1 && !fork_ev_) MG_CUDA(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
     dirty_ = false;
     return MG_OK;
 }
@@ -825,18 +854,16 @@ static uint32_t fault_tx_extra()
     return v > 0 && v < 4096 ? (uint32_t)v : 0u;
 }
 
-int Engine::launch_once()
+// One step of one lane on stream `st`: a launch group, or one generic job.
+int Engine::launch_lane(const Group& g, Job* generic_job, cudaStream_t st)
 {
-    for (Group& g : groups_) {
-        if (g.generic) {
-            for (Job* j : g.jobs) {
-                const unsigned blocks = (unsigned)((j->g.n + 255) / 256);
-                if (g.fp32) ch_step_generic_kernel<float><<<blocks, 256, 0, stream>>>(d_jobs_ + j->slot);
-                else ch_step_generic_kernel<double><<<blocks, 256, 0, stream>>>(d_jobs_ + j->slot);
-                ch_step_generic_finish<<<1, 32, 0, stream>>>(d_jobs_ + j->slot);
-            }
-            continue;
-        }
+    if (g.generic) {
+        Job* j = generic_job;
+        const unsigned blocks = (unsigned)((j->g.n + 255) / 256);
+        if (g.fp32) ch_step_generic_kernel<float><<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
+        else ch_step_generic_kernel<double><<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
+        ch_step_generic_finish<<<1, 32, 0, st>>>(d_jobs_ + j->slot);
+    } else {
         StepArgs a;
         a.jobs = d_jobs_;
         a.job_slot = g.d_slot;
@@ -848,9 +875,38 @@ int Engine::launch_once()
         a.spin_limit = spin_limit();
         a.err = d_err_;
         a.tx_extra = fault_tx_extra();
-        step_kernel(g.fp32, g.flat, g.nbuf, g.simple, g.block, g.mass, g.fixed_nx)<<<g.grid, g.block, g.smem, stream>>>(a);
+        step_kernel(g.fp32, g.flat, g.nbuf, g.simple, g.block, g.mass, g.fixed_nx)<<<g.grid, g.block, g.smem, st>>>(a);
     }
     MG_CUDA(cudaGetLastError());
+    return MG_OK;
+}
+
+// k steps of every job.  Lanes (launch groups; generic jobs one by one) hold
+// disjoint jobs, so with several lanes each runs its k steps on its own
+// stream, forked from and joined back into `stream`: small classes fill the
+// GPU beside large ones instead of after them.
+int Engine::launch_steps(int k)
+{
+    std::vector<std::pair<const Group*, Job*>> lanes;
+    for (const Group& g : groups_) {
+        if (g.generic)
+            for (Job* j : g.jobs) lanes.emplace_back(&g, j);
+        else
+            lanes.emplace_back(&g, nullptr);
+    }
+    if (lanes.size() <= 1) {
+        for (int i = 0; i < k; ++i)
+            for (auto& l : lanes) MG_TRY(launch_lane(*l.first, l.second, stream));
+        return MG_OK;
+    }
+    if (aux_.size() < lanes.size() || !fork_ev_) return fail(MG_ECUDA, "lane streams missing (engine not rebuilt)");
+    MG_CUDA(cudaEventRecord(fork_ev_, stream));
+    for (size_t i = 0; i < lanes.size(); ++i) {
+        MG_CUDA(cudaStreamWaitEvent(aux_[i], fork_ev_, 0));
+        for (int s = 0; s < k; ++s) MG_TRY(launch_lane(*lanes[i].first, lanes[i].second, aux_[i]));
+        MG_CUDA(cudaEventRecord(aux_ev_[i], aux_[i]));
+        MG_CUDA(cudaStreamWaitEvent(stream, aux_ev_[i], 0));
+    }
     return MG_OK;
 }
 
@@ -864,7 +920,7 @@ int Engine::graph_for(int k, cudaGraphExec_t* out)
     cudaGraph_t graph;
     MG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     int rc = MG_OK;
-    for (int i = 0; i < k && rc == MG_OK; ++i) rc = launch_once();
+    rc = launch_steps(k);
     cudaError_t e = cudaStreamEndCapture(stream, &graph);
     if (rc != MG_OK) {
         if (e == cudaSuccess) cudaGraphDestroy(graph);
@@ -904,7 +960,7 @@ int Engine::enqueue_steps(int nsteps)
             MG_CUDA(cudaGraphLaunch(ex, stream));
             nsteps -= k;
         } else {
-            MG_TRY(launch_once());
+            MG_TRY(launch_steps(1));
             nsteps -= 1;
         }
     }

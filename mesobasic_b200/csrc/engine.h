@@ -91,7 +91,7 @@ class Engine {
 
     // job lifetime: allocate buffers + maps, take a slot
     int add_job(const mg_ch_params& p, long long target, Job** out);
-    void remove_job(Job* j);  // frees everything of the job (caller synced)
+    void remove_job(Job* j);  // releases the job; its device memory is freed at the next rebuild
     int set_tiling(Job* j, const mg_tiling& t);
 
     int upload(Job* j, const double* host, long long target);  // resets step
@@ -105,6 +105,7 @@ class Engine {
     int nitems_total() const;
     int nctas_total() const;
     int nlaunch_per_step() const;
+    long long rebuilds() const { return rebuilds_; }  // launch-set rebuilds so far
 
     int device = 0;
     // jobs share launches (batch, server): tile every job for equally full
@@ -128,7 +129,14 @@ class Engine {
     };
     int rebuild();
     void free_groups();
-    int launch_once();
+    int launch_lane(const Group& g, Job* generic_job, cudaStream_t st);
+    int launch_steps(int k);
+    long long rebuilds_ = 0;
+    std::vector<void*> graveyard_;  // device buffers of removed jobs, freed by rebuild()
+    void free_graveyard();
+    std::vector<cudaStream_t> aux_;  // one per lane beyond the first (launch_steps)
+    std::vector<cudaEvent_t> aux_ev_;
+    cudaEvent_t fork_ev_ = nullptr;
     int graph_for(int k, cudaGraphExec_t* out);
     void drop_graphs();
     int to_double(Job* j, double* d_dst);   // current field -> device doubles

@@ -4,10 +4,11 @@
 // A worker thread owns one Engine.  Each tick it
 //   1. admits queued jobs, oldest first, that fit the HBM budget and a free
 //      slot (first fit: a large job at the head does not block small ones);
-//   2. enqueues k steps for every admitted job together -- one fused launch
-//      per precision class per step, all jobs' tiles in the same persistent
-//      grid -- where k is the fewest steps any admitted job still needs
-//      (capped), so finished jobs retire promptly;
+//   2. enqueues steps_per_tick steps for every admitted job together -- one
+//      fused launch per class per step, all jobs' tiles in the same
+//      persistent grid, classes side by side on their own streams; a job
+//      that reaches its step count stops on the device (its tiles skip), so
+//      ticks keep one length and one captured graph per job set;
 //   3. retires jobs that reached their step count: downloads the field and
 //      diagnostics, frees their memory, records the latency.
 // Per-job arithmetic does not depend on which other jobs share a launch:
@@ -41,7 +42,8 @@ struct ServerJob {
     mg::Job* job = nullptr;
     size_t bytes = 0;
     Clock::time_point t_submit, t_done;
-    std::vector<double> result;
+    std::unique_ptr<double[]> result;  // final field (not zero-filled first)
+    size_t result_n = 0;
     mg_ch_stats stats{};
     std::string error;
 };
@@ -67,6 +69,8 @@ struct mg_server {
     bool have_first = false;
     Clock::time_point t_first, t_last;
     double site_updates = 0;
+    double step_s = 0, admit_s = 0, retire_s = 0;  // worker time (see mg_server_stats)
+    long long ticks = 0;
 
     void run();
     void admit_locked();
@@ -114,8 +118,9 @@ void mg_server::admit_locked()
 void mg_server::retire(ServerJob* sj, bool ok, const char* why)
 {
     if (ok) {
-        sj->result.resize((size_t)sj->p.nx * sj->p.ny * sj->p.nz);
-        int rc = eng.download(sj->job, sj->result.data());
+        sj->result_n = (size_t)sj->p.nx * sj->p.ny * sj->p.nz;
+        sj->result.reset(new (std::nothrow) double[sj->result_n]);
+        int rc = sj->result ? eng.download(sj->job, sj->result.get()) : fail(MG_ENOMEM, "host allocation failed");
         if (rc == MG_OK) {
             rc = eng.diagnostics(sj->job, &sj->stats);
             if (rc == MG_ENONFINITE) rc = MG_OK;  // reported in stats.nonfinite
@@ -145,24 +150,38 @@ void mg_server::retire(ServerJob* sj, bool ok, const char* why)
     cv_done.notify_all();
 }
 
+static double seconds_since(Clock::time_point t0)
+{
+    return std::chrono::duration<double>(Clock::now() - t0).count();
+}
+
 void mg_server::run()
 {
     cudaSetDevice(eng.device);
     for (;;) {
         {
             std::unique_lock<std::mutex> lock(mu);
+            auto t0 = Clock::now();
             admit_locked();
+            admit_s += seconds_since(t0);
             while (running.empty()) {
                 if (stopping && queue.empty()) return;
                 cv_work.wait_for(lock, std::chrono::milliseconds(20));
+                t0 = Clock::now();
                 admit_locked();
+                admit_s += seconds_since(t0);
             }
         }
-        long long k = steps_per_tick;
-        for (ServerJob* sj : running) k = std::min(k, sj->nsteps - sj->done_steps);
-        k = std::max(k, 1LL);
+        const long long k = steps_per_tick;
+        const auto t0 = Clock::now();
         int rc = eng.enqueue_steps((int)k);
         if (rc == MG_OK) rc = eng.sync(600LL * 1000 * 1000);
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            step_s += seconds_since(t0);
+            ++ticks;
+        }
+        const auto t1 = Clock::now();
         std::vector<ServerJob*> snapshot = running;
         if (rc != MG_OK) {
             const std::string why = mg::last_error();
@@ -173,6 +192,8 @@ void mg_server::run()
             sj->done_steps = std::min(sj->nsteps, sj->done_steps + k);
             if (sj->done_steps >= sj->nsteps) retire(sj, true, nullptr);
         }
+        std::lock_guard<std::mutex> lock(mu);
+        retire_s += seconds_since(t1);
     }
 }
 
@@ -256,7 +277,7 @@ int mg_server_result(mg_server_t* s, long long job_id, long long timeout_us, dou
         s->jobs.erase(it);
         return fail(MG_EDEVICE, "job %lld failed: %s", job_id, why.c_str());
     }
-    if (field_out) std::copy(sj->result.begin(), sj->result.end(), field_out);
+    if (field_out) std::copy(sj->result.get(), sj->result.get() + sj->result_n, field_out);
     if (stats) *stats = sj->stats;
     s->jobs.erase(it);
     return MG_OK;
@@ -272,6 +293,11 @@ int mg_server_stats_get(mg_server_t* s, mg_server_stats* out)
     st.completed = s->completed;
     st.failed = s->failed;
     st.running = (long long)s->running.size();
+    st.step_s = s->step_s;
+    st.admit_s = s->admit_s;
+    st.retire_s = s->retire_s;
+    st.ticks = s->ticks;
+    st.rebuilds = s->eng.rebuilds();
     st.queued = (long long)s->queue.size();
     if (!s->latencies_ms.empty()) {
         std::vector<double> v = s->latencies_ms;
