@@ -236,3 +236,26 @@ def test_autotune_picks_a_valid_tiling_with_identical_results(oracle, tmp_path, 
     ic = oracle.ic((64, 32, 32), 0.0, 0.2, False, 3)
     assert np.array_equal(run_gpu(p, ic, 10, tiling=t), oracle.run(ic, (64, 32, 32), (1, 1, 1), 0.005, 1, 1, 10))
     assert (tmp_path / "tune.json").exists()
+
+
+# 256-wide rows take the fixed-width kernel variants (row width a compile-
+# time constant); the chunk counts vary the planes per tile and the tail of
+# the three-plane register rotation.
+@pytest.mark.parametrize("ty,nchunk,nbuf", [(5, 1, 4), (7, 2, 4), (6, 3, 4), (4, 5, 4), (8, 7, 4),
+                                            (5, 1, 8), (6, 3, 8), (4, 5, 8), (3, 7, 8)])
+def test_fixed_width_fp64_bit_identical_to_oracle(oracle, ty, nchunk, nbuf):
+    dims = (256, 18, 23)
+    ic = oracle.ic(dims, 0.05, 0.3, False, 17)
+    want = oracle.run(ic, dims, (1.0, 1.0, 1.0), 0.005, 1.0, 1.3, 6)
+    got = run_gpu(mb.make_params(*dims, 0.005, kappa=1.3), ic, 6, tiling=(ty, nchunk, nbuf, 0))
+    assert np.array_equal(got, want), np.abs(got - want).max()
+
+
+@pytest.mark.parametrize("mc", [0, 1])
+def test_fixed_width_fp32_within_tolerance(oracle, mc):
+    dims = (256, 16, 21)
+    ic = oracle.ic(dims, 0.3, 0.02, True, 5)
+    want = oracle.run(ic, dims, (1.0, 1.0, 1.0), 0.005, 1.0, 1.5, 100)
+    for t in [(6, 3, 4, 0), (5, 2, 8, 0)]:
+        got = run_gpu(mb.make_params(*dims, 0.005, kappa=1.5, precision="fp32", mass_correct=mc), ic, 100, tiling=t)
+        assert np.abs(got - want).max() <= 1e-4, (t, np.abs(got - want).max())
