@@ -106,6 +106,14 @@ int mg_ch_sync(mg_ch_t* h, long long timeout_us);
  * read of c in outputPhaseField -> SfieldFD::writeVTKFile (SfieldFD.cpp:363-430). */
 int mg_ch_get_field(mg_ch_t* h, double* host);
 
+/* Appends the current field to `path` as one legacy-VTK block (header +
+ * "%.3f" lines, x fastest, skip rules), byte-identical to mg_vtk_write of
+ * the downloaded field, but formatted on the GPU: only the text crosses to
+ * the host.  Values of magnitude >= 4e12 give MG_EINVAL (mg_vtk_write takes
+ * any value).  Waits for enqueued work.  Replaces: SfieldFD::writeVTKFile
+ * (SfieldFD.cpp:363-430) called from outputPhaseField. */
+int mg_ch_write_vtk(mg_ch_t* h, const char* path, const char* tag, int iskip, int jskip, int kskip);
+
 /* Mass/energy diagnostics of the current field.  No reference counterpart
  * (the reference logs neither).  Returns MG_ENONFINITE if any site is not
  * finite (stats are still filled). */

@@ -96,6 +96,10 @@ class CHSim:
     def get_field_ptr(self, host_ptr: int):
         check(self._L.mg_ch_get_field(self._h, ctypes.cast(host_ptr, ctypes.POINTER(ctypes.c_double))))
 
+    def write_vtk(self, path, tag="c", iskip=1, jskip=1, kskip=1):
+        """Appends the current field as legacy VTK, formatted on the GPU."""
+        check(self._L.mg_ch_write_vtk(self._h, str(path).encode(), tag.encode(), iskip, jskip, kskip))
+
     def reduce(self, allow_nonfinite: bool = False) -> dict:
         st = Stats()
         rc = self._L.mg_ch_reduce(self._h, ctypes.byref(st))

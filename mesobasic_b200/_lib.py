@@ -81,6 +81,7 @@ SIGNATURES = {
     "mg_ch_sync": (ctypes.c_int, [_vp, ctypes.c_longlong]),
     "mg_ch_get_field": (ctypes.c_int, [_vp, _dp]),
     "mg_ch_reduce": (ctypes.c_int, [_vp, _P(Stats)]),
+    "mg_ch_write_vtk": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "mg_ch_structure_factor": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp, _dp]),
     "mg_ch_stream": (_vp, [_vp]),
     "mg_ch_field_device": (_vp, [_vp]),

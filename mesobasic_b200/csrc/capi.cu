@@ -71,6 +71,13 @@ int mg_ch_get_field(mg_ch_t* h, double* host)
     return h->eng.download(h->job, host);
 }
 
+int mg_ch_write_vtk(mg_ch_t* h, const char* path, const char* tag, int iskip, int jskip, int kskip)
+{
+    mg::clear_error();
+    if (!h) return fail(MG_EINVAL, "null handle");
+    return h->eng.write_vtk(h->job, path, tag, iskip, jskip, kskip);
+}
+
 int mg_ch_reduce(mg_ch_t* h, mg_ch_stats* out)
 {
     mg::clear_error();

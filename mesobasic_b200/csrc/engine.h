@@ -97,6 +97,8 @@ class Engine {
     int upload(Job* j, const double* host, long long target);  // resets step
     int download(Job* j, double* host);                         // syncs
     int diagnostics(Job* j, mg_ch_stats* out);                  // syncs
+    // appends the job's current field as legacy VTK, formatted on the GPU (vtk_device.cu)
+    int write_vtk(Job* j, const char* path, const char* tag, int iskip, int jskip, int kskip);
     int structure_factor(Job* j, int nbins, double* k, double* S, double* k1);
     int enqueue_steps(int nsteps);  // all jobs, one launch group set per step
     int sync(long long timeout_us);

@@ -12,6 +12,25 @@
 namespace mg {
 int fail(int code, const char* fmt, ...);
 void clear_error();
+
+// The header block of SfieldFD::writeVTKFile (SfieldFD.cpp:383-399) for a
+// single rank; shared by the host and device writers.
+void vtk_header(FILE* f, const char* tag, int nx, int ny, int nz, int iskip, int jskip, int kskip)
+{
+    const char* d = "   ";
+    std::fprintf(f, "# vtk DataFile Version 3.1\n");
+    std::fprintf(f, "VTK file containing grid data\n");
+    std::fprintf(f, "ASCII\n");
+    std::fprintf(f, " \n");
+    std::fprintf(f, "DATASET STRUCTURED_POINTS\n");
+    std::fprintf(f, "DIMENSIONS%s%d%s%d%s%d\n", d, nx / iskip, d, ny / jskip, d, nz / kskip);
+    std::fprintf(f, "ORIGIN %s0%s0%s0\n", d, d, d);
+    std::fprintf(f, "SPACING%s%g%s%g%s%g\n", d, 1.0 * iskip, d, 1.0 * jskip, d, 1.0 * kskip);
+    std::fprintf(f, " \n");
+    std::fprintf(f, "POINT_DATA %d\n", (nx / iskip) * (ny / jskip) * (nz / kskip));
+    std::fprintf(f, "SCALARS %s float\n", tag);
+    std::fprintf(f, "LOOKUP_TABLE default\n");
+}
 }  // namespace mg
 
 namespace {
@@ -93,19 +112,7 @@ int mg_vtk_write(const char* path, const char* tag, const double* field, const i
     if (!f) return mg::fail(MG_EINVAL, "cannot open %s for appending", path);
     std::vector<char> iobuf(1 << 20);
     std::setvbuf(f, iobuf.data(), _IOFBF, iobuf.size());
-    const char* d = "   ";
-    std::fprintf(f, "# vtk DataFile Version 3.1\n");
-    std::fprintf(f, "VTK file containing grid data\n");
-    std::fprintf(f, "ASCII\n");
-    std::fprintf(f, " \n");
-    std::fprintf(f, "DATASET STRUCTURED_POINTS\n");
-    std::fprintf(f, "DIMENSIONS%s%d%s%d%s%d\n", d, nx / iskip, d, ny / jskip, d, nz / kskip);
-    std::fprintf(f, "ORIGIN %s0%s0%s0\n", d, d, d);
-    std::fprintf(f, "SPACING%s%g%s%g%s%g\n", d, 1.0 * iskip, d, 1.0 * jskip, d, 1.0 * kskip);
-    std::fprintf(f, " \n");
-    std::fprintf(f, "POINT_DATA %d\n", (nx / iskip) * (ny / jskip) * (nz / kskip));
-    std::fprintf(f, "SCALARS %s float\n", tag);
-    std::fprintf(f, "LOOKUP_TABLE default\n");
+    mg::vtk_header(f, tag, nx, ny, nz, iskip, jskip, kskip);
     char line[64];
     for (int k = 1; k < nz + 1; k += kskip)
         for (int j = 1; j < ny + 1; j += jskip) {

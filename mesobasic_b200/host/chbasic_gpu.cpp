@@ -90,18 +90,18 @@ void CHBasicGPU::getField(std::vector<double>& out)
 
 void CHBasicGPU::outputPhaseField()
 {
-    if (!vtk && dump_prefix.empty()) return;
-    std::vector<double> c;
-    getField(c);
     if (vtk) {
         // SfieldFD::writeVTKFile names the file vtkoutput/<tag>_<step>.vtk
-        // and appends to it (SfieldFD.cpp:363-430)
+        // and appends to it (SfieldFD.cpp:363-430); the text is formatted on
+        // the GPU
+        flush();
         char path[64];
         std::snprintf(path, sizeof path, "vtkoutput/c_%d.vtk", current_step);
-        const int dims[3] = {gp.nx, gp.ny, gp.nz};
-        check(mg_vtk_write(path, "c", c.data(), dims, p.iskip, p.jskip, p.kskip), "mg_vtk_write");
+        check(mg_ch_write_vtk(h, path, "c", p.iskip, p.jskip, p.kskip), "mg_ch_write_vtk");
     }
     if (!dump_prefix.empty()) {
+        std::vector<double> c;
+        getField(c);
         // raw dump: int32 {xOff, nx, ny, nz, step}, then the field as
         // float64, dense x-fastest
         char name[512];
