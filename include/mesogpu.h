@@ -52,6 +52,12 @@ typedef struct {
                               2^-23 on a window of sites that moves every step,
                               so rounding errors of the field do not accumulate
                               as a drift of total mass */
+    double noise;          /* >0: after each step every site gets
+                              c += dt * (noise * (u - 0.5)), u uniform in (0,1)
+                              [PFApp/noiseStr] (TIPSphil.cpp:200-209); 0: off */
+    unsigned long long noise_seed; /* key of the counter-based generator
+                              (Philox4x32-10): u depends on (seed, site, step)
+                              only, so it is the same alone, batched or served */
 } mg_ch_params;
 
 typedef struct {

@@ -24,11 +24,12 @@ __all__ = ["CHSim", "Batch", "Server", "Params", "Stats", "Tiling", "MGError", "
 
 
 def make_params(nx, ny, nz, dt, kappa=1.0, M=1.0, dx=1.0, dy=1.0, dz=1.0, bc=(1, 1, 1),
-                precision="fp64", mass_correct=None) -> Params:
+                precision="fp64", mass_correct=None, noise=0.0, noise_seed=0) -> Params:
     prec = MG_FP32 if precision in ("fp32", MG_FP32) else MG_FP64
     if mass_correct is None:
         mass_correct = 1 if prec == MG_FP32 else 0
-    return Params(nx, ny, nz, dx, dy, dz, dt, M, kappa, bc[0], bc[1], bc[2], prec, int(mass_correct))
+    return Params(nx, ny, nz, dx, dy, dz, dt, M, kappa, bc[0], bc[1], bc[2], prec, int(mass_correct), float(noise),
+                  int(noise_seed))
 
 
 def _dims(p: Params):

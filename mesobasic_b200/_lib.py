@@ -36,7 +36,8 @@ class Params(ctypes.Structure):
                 ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
                 ("dt", ctypes.c_double), ("M", ctypes.c_double), ("kappa", ctypes.c_double),
                 ("bx", ctypes.c_int), ("by", ctypes.c_int), ("bz", ctypes.c_int),
-                ("precision", ctypes.c_int), ("mass_correct", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("mass_correct", ctypes.c_int),
+                ("noise", ctypes.c_double), ("noise_seed", ctypes.c_ulonglong)]
 
 
 class Stats(ctypes.Structure):

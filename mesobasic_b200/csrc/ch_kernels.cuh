@@ -803,6 +803,73 @@ __global__ void ch_step_generic_kernel(JobDev* job)
     out[s] = A::add(c[s], A::mul(lap, T(J.dtM)));
 }
 
+// ---------------------------------------------------------------------------
+// Per-step noise, the random fluctuation term of TIPSphil::updatePhaseField
+// (TIPSphil.cpp:200-209): after a step every site gets c += dt*(noise*(r -
+// 0.5)), each product rounded on its own as there.  The reference draws r
+// from rand(); here r comes from Philox4x32-10 (Salmon, Moraes, Dror, Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC 2011), keyed by the
+// job's seed, with counter (site / 4, step): four sites per draw, r =
+// (word + 0.5) * 2^-32, so r depends on (seed, site, step) only.
+
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r) {
+            k.x += 0x9E3779B9u;
+            k.y += 0xBB67AE85u;
+        }
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    }
+    return c;
+}
+
+// Adds the noise of the step just taken (the job's step counter) once: a
+// replayed graph step that skipped the job leaves noise_step == step, and
+// the blocks return.  The last block to finish records the step.
+template <typename T>
+__global__ void ch_noise_kernel(JobDev* job)
+{
+    __shared__ long long st;
+    __shared__ int go;
+    JobDev* J = job;
+    if (threadIdx.x == 0) {
+        st = *((volatile long long*)&J->step);
+        go = st > *((volatile long long*)&J->noise_step);
+    }
+    __syncthreads();
+    if (!go) return;
+    T* c = static_cast<T*>(J->buf[st & 1]);
+    const long long n = (long long)J->nx * J->ny * J->nz;
+    const double noise = J->noise, dt = J->dtM_dt;
+    const uint2 key = make_uint2((uint32_t)J->noise_seed, (uint32_t)(J->noise_seed >> 32));
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; 4 * g < n; g += (long long)gridDim.x * blockDim.x) {
+        const uint4 w = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)(g >> 32), (uint32_t)st, (uint32_t)(st >> 32)), key);
+        const uint32_t word[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const long long s = 4 * g + e;
+            if (s >= n) break;
+            const double r = __dadd_rn(__dmul_rn((double)word[e], 2.3283064365386963e-10), 1.1641532182693481e-10);
+            const double val = __dmul_rn(noise, __dsub_rn(r, 0.5));
+            const double inc = __dmul_rn(dt, val);
+            if constexpr (sizeof(T) == 8) c[s] = __dadd_rn(c[s], inc);
+            else c[s] = c[s] + (float)inc;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&J->noise_done, 1u) == gridDim.x - 1) {
+            J->noise_step = st;
+            J->noise_done = 0;
+        }
+    }
+}
+
 // advances the step counter after a generic-path step
 __global__ void ch_step_generic_finish(JobDev* job)
 {
@@ -819,6 +886,8 @@ __global__ void ch_job_reset(JobDev* job, long long target)
         job->err = 0;
         job->nudge_begin = 0;
         job->nudge_count = 0;
+        job->noise_step = 0;
+        job->noise_done = 0;
     }
 }
 

@@ -60,11 +60,16 @@ struct alignas(16) JobDev {
     int bw;                     // TMA box width = shared-memory piece width
     double cx, cy, cz;          // 1/d^2 (multiply) or d^2 (divide when JF_DIV_*)
     double kap, dtM;            // kappa, dt*M
+    double dtM_dt;              // dt (the noise term's factor)
     double inv_nsites;          // 1 / (nx*ny*nz)
     double mass_target;         // sum(c) of the uploaded field (JF_MASS)
     long long nudge_begin;      // first site of the next step's nudge window (JF_MASS)
     long long nudge_count;      // sites in the window; the sign is the nudge's
     double mass_last;           // sum(c) after the last step (JF_MASS)
+    double noise;               // per-step noise strength (0: none)
+    unsigned long long noise_seed;
+    long long noise_step;       // the last step whose noise has been added
+    unsigned int noise_done;    // blocks of the running noise launch finished
     long long step;             // steps taken
     long long target;           // the job stops stepping here
     unsigned int done;          // items finished in the running launch

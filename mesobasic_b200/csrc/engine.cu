@@ -120,6 +120,7 @@ int validate_params(const mg_ch_params& p)
         return fail(MG_EINVAL, "bx, by, bz must be 0 (no-flux) or 1 (periodic)");
     if (p.precision != MG_FP64 && p.precision != MG_FP32) return fail(MG_EINVAL, "precision must be MG_FP64 or MG_FP32");
     if (p.mass_correct && p.precision != MG_FP32) return fail(MG_EINVAL, "mass_correct applies to MG_FP32 only");
+    if (!(p.noise >= 0) || !std::isfinite(p.noise)) return fail(MG_EINVAL, "noise must be finite and >= 0");
     return MG_OK;
 }
 
@@ -525,6 +526,9 @@ static void fill_jobdev(const Job& j, JobDev* jd)
     jd->flags = flags;
     jd->kap = j.p.kappa;
     jd->dtM = j.p.dt * j.p.M;
+    jd->dtM_dt = j.p.dt;
+    jd->noise = j.p.noise;
+    jd->noise_seed = j.p.noise_seed;
     jd->inv_nsites = 1.0 / (double)g.n;
     jd->target = j.target < 0 ? LLONG_MAX : j.target;
 }
@@ -877,6 +881,16 @@ int Engine::launch_lane(const Group& g, Job* generic_job, cudaStream_t st)
         a.tx_extra = fault_tx_extra();
         step_kernel(g.fp32, g.flat, g.nbuf, g.simple, g.block, g.mass, g.fixed_nx)<<<g.grid, g.block, g.smem, st>>>(a);
     }
+    // the noise term, per job that has one, after the step
+    auto noise = [&](Job* j) {
+        if (!(j->p.noise > 0)) return;
+        const unsigned blocks = (unsigned)std::min<long long>((j->g.n / 4 + 256) / 256, 8LL * info.sms);
+        if (g.fp32) ch_noise_kernel<float><<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
+        else ch_noise_kernel<double><<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
+    };
+    if (g.generic) noise(generic_job);
+    else
+        for (Job* j : g.jobs) noise(j);
     MG_CUDA(cudaGetLastError());
     return MG_OK;
 }

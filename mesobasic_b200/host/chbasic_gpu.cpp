@@ -34,6 +34,10 @@ CHBasicGPU::CHBasicGPU(const CommonParams& pin, const InputFile& in) : p(pin)
     if (prec != "fp64" && prec != "fp32") throw std::invalid_argument("PFApp/precision must be fp64 or fp32");
     gp.precision = prec == "fp32" ? MG_FP32 : MG_FP64;
     gp.mass_correct = gp.precision == MG_FP32 ? in("PFApp/mass_correct", 1) : 0;
+    // the reference's per-step fluctuation term (TIPSphil.cpp:200-209); off
+    // by default in the plain Cahn-Hilliard model
+    gp.noise = in("PFApp/noiseStr", 0.0);
+    gp.noise_seed = (unsigned long long)in("PFApp/noise_seed", in("PFApp/seed", 42));
     co = in("PFApp/co", 0.0);
     noise_amp = in("PFApp/noise_amp", 0.1);
     noise_type = in("PFApp/noise_type", "uniform");

@@ -18,6 +18,8 @@
 // Keys of this build only:
 //   precision      fp64 (bit-identical to the reference build) | fp32   fp64
 //   mass_correct   fp32: FP64 mass feedback each step             1
+//   noiseStr       per-step noise c += dt*noiseStr*(u - 0.5)       0 (off)
+//   noise_seed     key of the noise generator                      seed
 //   device         CUDA device                                     0
 //
 // updatePhaseField only counts the step: pending steps are enqueued

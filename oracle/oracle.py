@@ -224,3 +224,33 @@ def vtk_text(c, dims, tag, iskip=1, jskip=1, kskip=1) -> str:
             row = a[k - 1, j - 1]
             lines.extend(f"{row[i - 1]:.3f}" for i in xs)
     return "\n".join(lines) + "\n"
+
+
+# --------------------------------------------------------------- noise term
+PHILOX_M = (0xD2511F53, 0xCD9E8D57)
+PHILOX_W = (0x9E3779B9, 0xBB67AE85)
+
+
+def philox4x32_10(ctr, key):
+    """Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC 2011) on Python ints:
+    counter of four 32-bit words, key of two; returns four 32-bit words."""
+    c, k = list(ctr), list(key)
+    for r in range(10):
+        if r:
+            k = [(k[0] + PHILOX_W[0]) & 0xFFFFFFFF, (k[1] + PHILOX_W[1]) & 0xFFFFFFFF]
+        p0, p1 = PHILOX_M[0] * c[0], PHILOX_M[1] * c[2]
+        c = [(p1 >> 32) ^ c[1] ^ k[0], p1 & 0xFFFFFFFF, (p0 >> 32) ^ c[3] ^ k[1], p0 & 0xFFFFFFFF]
+    return c
+
+
+def noise_increments(n, step, seed, noise, dt):
+    """dt * (noise * (r - 0.5)) per site, r = (word + 0.5) * 2^-32 with the
+    word for site s from philox4x32_10((s//4, 0, step, 0) split into 32-bit
+    halves, seed) -- the per-step fluctuation term of TIPSphil.cpp:200-209
+    with a counter-based generator in place of rand()."""
+    key = (seed & 0xFFFFFFFF, seed >> 32)
+    words = np.empty(4 * ((n + 3) // 4), dtype=np.float64)
+    for g in range(len(words) // 4):
+        words[4 * g:4 * g + 4] = philox4x32_10((g & 0xFFFFFFFF, g >> 32, step & 0xFFFFFFFF, step >> 32), key)
+    r = words[:n] * 2.3283064365386963e-10 + 1.1641532182693481e-10
+    return dt * (noise * (r - 0.5))

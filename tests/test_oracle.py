@@ -121,3 +121,11 @@ def test_structure_factor_peak_of_single_mode(oracle):
     c = np.cos(k * x)[None, None, :] * np.ones((1, ny, 1))
     kc, s, cnt, k1 = oracle.structure_factor(c, (nx, ny, 1))
     assert abs(k1 - k) < 1e-12
+
+
+def test_philox_known_answers(oracle):
+    # the published known-answer vectors of Philox4x32-10
+    assert oracle.philox4x32_10([0, 0, 0, 0], [0, 0]) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    assert oracle.philox4x32_10([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2) == [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]
+    assert oracle.philox4x32_10([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0]) == \
+        [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
