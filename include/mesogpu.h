@@ -148,6 +148,40 @@ int mg_ch_set_tiling(mg_ch_t* h, const mg_tiling* t);
 /* Frees the device buffers.  Replaces: PFApp::~PFApp (PFApp.cpp:69-72). */
 void mg_ch_destroy(mg_ch_t* h);
 
+/* ----------------------------------------------------------------------
+ * Variable mobility: the TIPSphil model (Flory-Huggins chemical potential,
+ * Phillies mobility, div(mob grad mu) with harmonic-mean face mobilities).
+ * -------------------------------------------------------------------- */
+
+/* Keys of the reference input file in brackets, the reference defaults in
+ * parentheses (TIPSphil.cpp:41-59). */
+typedef struct {
+    double alpha, beta;     /* chi = alpha/T + beta [PFApp/alpha (1), beta (1)] */
+    double N;               /* polymer length [PFApp/N (100)] */
+    double A;               /* c <= 0 branch of mu [PFApp/A (1)] */
+    double Tinit, Tbath;    /* linear quench Tinit -> Tbath over nstep [PFApp/Tinit, Tbath (273)] */
+    double Tcrystal;        /* mobility x 0.001 at or below it [PFApp/Tcrystal (273)] */
+    double nu, gamma;       /* Phillies law D*exp(-gamma*phi^nu) [PFApp/nu (1), gamma (10)] */
+    double D0;              /* diffusivity and mobility cap [PFApp/D0 (1e-7)] */
+    double Mweight, Mvolume;/* phi -> g/L [PFApp/Mweight (100), Mvolume (0.1)] */
+    long long nstep;        /* steps of the quench [Time/nstep] */
+} mg_fh_params;
+
+/* A simulation stepped by the variable-mobility update of
+ * TIPSphil::updatePhaseField (TIPSphil.cpp:113-211) instead of the constant-
+ * mobility Cahn-Hilliard step: FP64 only (params->precision MG_FP64,
+ * mass_correct 0); kappa is [PFApp/kap]; params->M is unused (the mobility
+ * comes from the model); params->noise adds the reference's fluctuation term
+ * (TIPSphil.cpp:200-209, [PFApp/noiseStr]).  Every other mg_ch_* call
+ * applies.  Replaces: PFBaseClass::PFFactory returning TIPSphil
+ * (PFBaseClass.cpp:43). */
+int mg_fh_create(const mg_ch_params* params, const mg_fh_params* fh, int device, mg_ch_t** out);
+
+/* The mobility field of the last step taken (nx*ny*nz doubles, x fastest;
+ * waits for enqueued work).  Replaces: the mob field TIPSphil writes at
+ * PFApp/mobStep (TIPSphil.cpp:180-185). */
+int mg_fh_mobility(mg_ch_t* h, double* host);
+
 /* Times candidate decompositions of `params` on `device` (scratch fields,
  * `trials` timed launches each) and returns the fastest.  Results are
  * cached per (shape, precision) in the process and, when the environment

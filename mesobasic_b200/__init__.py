@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (MG_FP32, MG_FP64, MG_JOB_DONE, MG_JOB_FAILED, MG_JOB_QUEUED, MG_JOB_RUNNING, MGError,
-                   Params, ServerStats, Stats, Tiling, check, load)
+                   FhParams, Params, ServerStats, Stats, Tiling, check, load)
 
 __all__ = ["CHSim", "Batch", "Server", "Params", "Stats", "Tiling", "MGError", "MG_FP32", "MG_FP64",
            "make_params", "ic_generate", "vtk_write", "autotune", "load"]
@@ -47,15 +47,40 @@ def _dptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
-class CHSim:
-    """One simulation on one GPU."""
+# the reference TIPSphil constructor's defaults (TIPSphil.cpp:41-59)
+FH_DEFAULTS = dict(alpha=1.0, beta=1.0, N=100.0, A=1.0, Tinit=273.0, Tbath=273.0, Tcrystal=273.0, nu=1.0,
+                   gamma=10.0, D0=1e-7, Mweight=100.0, Mvolume=0.1)
 
-    def __init__(self, params: Params, device: int = 0):
+
+def make_fh_params(nstep, **kw) -> FhParams:
+    """Variable-mobility (TIPSphil) parameters; unnamed ones take the
+    reference's defaults."""
+    unknown = set(kw) - set(FH_DEFAULTS)
+    if unknown:
+        raise ValueError(f"unknown variable-mobility parameters {sorted(unknown)}")
+    v = dict(FH_DEFAULTS, **kw)
+    return FhParams(*(float(v[k]) for k in FH_DEFAULTS), int(nstep))
+
+
+class CHSim:
+    """One simulation on one GPU: the Cahn-Hilliard step, or with `fh`
+    (make_fh_params) the variable-mobility TIPSphil step."""
+
+    def __init__(self, params: Params, device: int = 0, fh: FhParams = None):
         self._L = load()
         self.params = params
         h = ctypes.c_void_p()
-        check(self._L.mg_ch_create(ctypes.byref(params), device, ctypes.byref(h)))
+        if fh is None:
+            check(self._L.mg_ch_create(ctypes.byref(params), device, ctypes.byref(h)))
+        else:
+            check(self._L.mg_fh_create(ctypes.byref(params), ctypes.byref(fh), device, ctypes.byref(h)))
         self._h = h
+
+    def mobility(self) -> np.ndarray:
+        """Mobility field of the last step (variable-mobility jobs)."""
+        out = np.empty(self.shape, dtype=np.float64)
+        check(self._L.mg_fh_mobility(self._h, _dptr(out)))
+        return out
 
     def close(self):
         if getattr(self, "_h", None):

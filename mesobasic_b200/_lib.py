@@ -40,6 +40,13 @@ class Params(ctypes.Structure):
                 ("noise", ctypes.c_double), ("noise_seed", ctypes.c_ulonglong)]
 
 
+class FhParams(ctypes.Structure):
+    _fields_ = [("alpha", ctypes.c_double), ("beta", ctypes.c_double), ("N", ctypes.c_double), ("A", ctypes.c_double),
+                ("Tinit", ctypes.c_double), ("Tbath", ctypes.c_double), ("Tcrystal", ctypes.c_double),
+                ("nu", ctypes.c_double), ("gamma", ctypes.c_double), ("D0", ctypes.c_double),
+                ("Mweight", ctypes.c_double), ("Mvolume", ctypes.c_double), ("nstep", ctypes.c_longlong)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("mass", ctypes.c_double), ("energy", ctypes.c_double), ("abs_mass", ctypes.c_double),
                 ("max_abs", ctypes.c_double), ("nonfinite", ctypes.c_longlong), ("step", ctypes.c_longlong)]
@@ -90,6 +97,8 @@ SIGNATURES = {
     "mg_ch_get_tiling": (ctypes.c_int, [_vp, _P(Tiling)]),
     "mg_ch_set_tiling": (ctypes.c_int, [_vp, _P(Tiling)]),
     "mg_ch_destroy": (None, [_vp]),
+    "mg_fh_create": (ctypes.c_int, [_P(Params), _P(FhParams), ctypes.c_int, _P(_vp)]),
+    "mg_fh_mobility": (ctypes.c_int, [_vp, _dp]),
     "mg_autotune": (ctypes.c_int, [_P(Params), ctypes.c_int, ctypes.c_int, _P(Tiling), _dp]),
     "mg_ic_generate": (ctypes.c_int, [_i3, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_uint, _dp]),
     "mg_vtk_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, _dp, _i3, ctypes.c_int, ctypes.c_int,

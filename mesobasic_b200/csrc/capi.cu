@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <cstdlib>
 #include <memory>
 #include <new>
@@ -41,6 +42,34 @@ int mg_ch_create(const mg_ch_params* params, int device, mg_ch_t** out)
     MG_TRY(h->eng.add_job(*params, -1, &h->job));
     *out = h.release();
     return MG_OK;
+}
+
+int mg_fh_create(const mg_ch_params* params, const mg_fh_params* fh, int device, mg_ch_t** out)
+{
+    mg::clear_error();
+    if (!params || !fh || !out) return fail(MG_EINVAL, "null argument");
+    *out = nullptr;
+    const double v[12] = {fh->alpha, fh->beta, fh->N, fh->A, fh->Tinit, fh->Tbath, fh->Tcrystal, fh->nu, fh->gamma,
+                          fh->D0, fh->Mweight, fh->Mvolume};
+    for (double x : v)
+        if (!std::isfinite(x)) return fail(MG_EINVAL, "variable-mobility parameters must be finite");
+    if (fh->nstep < 1) return fail(MG_EINVAL, "nstep must be >= 1");
+    if (fh->N == 0 || fh->Mvolume == 0 || fh->Tinit == 0) return fail(MG_EINVAL, "N, Mvolume and Tinit must be nonzero");
+    mg::Geometry g;
+    MG_TRY(mg::make_geometry(*params, &g));
+    std::unique_ptr<mg_ch> h(new (std::nothrow) mg_ch);
+    if (!h) return fail(MG_ENOMEM, "host allocation failed");
+    MG_TRY(h->eng.init(device, 1));
+    MG_TRY(h->eng.add_job(*params, -1, &h->job, fh));
+    *out = h.release();
+    return MG_OK;
+}
+
+int mg_fh_mobility(mg_ch_t* h, double* host)
+{
+    mg::clear_error();
+    if (!h) return fail(MG_EINVAL, "null handle");
+    return h->eng.mobility(h->job, host);
 }
 
 int mg_ch_set_field(mg_ch_t* h, const double* host)

@@ -870,6 +870,122 @@ __global__ void ch_noise_kernel(JobDev* job)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Variable-mobility step of TIPSphil::updatePhaseField (TIPSphil.cpp:113-211),
+// FP64, every operation rounded on its own in the reference's order; log,
+// exp, pow and sqrt are CUDA's (within an ulp or two of the host's libm).
+// Pass 1 stores mu and the mobility of every site; pass 2 forms the
+// harmonic-mean Laplacian of SfieldFD::Laplacian(const SfieldFD&)
+// (SfieldFD.cpp:333-355) and updates c.  Boundaries as the reference's
+// updateBoundaries: periodic axes wrap, a no-flux neighbour is the site itself.
+
+__device__ __forceinline__ int fh_at(int x, int y, int z, const JobDev& J)
+{
+    return (z * J.ny + y) * J.nx + x;
+}
+
+__global__ void fh_mu_mob_kernel(JobDev* job)
+{
+    using A = Arith<double>;
+    const JobDev& J = *job;
+    const FhDev& F = *J.fh;
+    const int nx = J.nx, ny = J.ny, nz = J.nz;
+    const size_t n = (size_t)nx * ny * nz;
+    const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (J.step >= J.target || s >= n) return;
+    const double* __restrict__ c = static_cast<const double*>(J.buf[J.step & 1]);
+    // temperature of the step being taken (PFApp passes it as current_step)
+    const double cs = (double)(J.step + 1);
+    const double T = A::sub(F.Tinit, A::mul(A::sub(F.Tinit, F.Tbath), A::div(cs, (double)F.nstep)));
+    const double kT = A::div(T, 273.0);
+    const double chi = A::add(A::div(F.alpha, T), F.beta);
+    const int x = (int)(s % nx), y = (int)((s / nx) % ny), z = (int)(s / ((size_t)nx * ny));
+    const bool pX = J.flags & JF_PER_X, pY = J.flags & JF_PER_Y, pZ = J.flags & JF_PER_Z;
+    const double cc = c[s];
+    const double xp = c[fh_at(wrap_or_clamp(x + 1, nx, pX), y, z, J)], xm = c[fh_at(wrap_or_clamp(x - 1, nx, pX), y, z, J)];
+    const double zp = c[fh_at(x, y, wrap_or_clamp(z + 1, nz, pZ), J)], zm = c[fh_at(x, y, wrap_or_clamp(z - 1, nz, pZ), J)];
+    double lapc;
+    if (J.flags & JF_FLAT) {
+        lapc = A::add(axis_term(xp, xm, cc, J.cx, J.flags & JF_DIV_X), axis_term(zp, zm, cc, J.cz, J.flags & JF_DIV_Z));
+    } else {
+        const double yp = c[fh_at(x, wrap_or_clamp(y + 1, ny, pY), z, J)], ym = c[fh_at(x, wrap_or_clamp(y - 1, ny, pY), z, J)];
+        lapc = A::add(A::add(axis_term(xp, xm, cc, J.cx, J.flags & JF_DIV_X), axis_term(yp, ym, cc, J.cy, J.flags & JF_DIV_Y)),
+                      axis_term(zp, zm, cc, J.cz, J.flags & JF_DIV_Z));
+    }
+    // chemical potential: df = ((log(cc)+1)/N - log(1-cc) - 1 + chi*(1-2cc)) * kT
+    double df = A::add(A::sub(A::sub(A::div(A::add(log(cc), 1.0), F.N), log(A::sub(1.0, cc))), 1.0),
+                       A::mul(chi, A::sub(1.0, A::mul(2.0, cc))));
+    df = A::mul(df, kT);
+    if (cc <= 0.0) df = A::mul(A::mul(-1.5, F.A), sqrt(-cc));
+    F.mu[s] = A::sub(df, A::mul(J.kap, lapc));
+    // Phillies self-diffusion over the second derivative of the free energy
+    double cc_phil, ddf;
+    if (cc >= 1.0) {
+        cc_phil = A::div(A::mul(1.0, F.Mweight), F.Mvolume);
+        ddf = A::mul(0.5, A::add(A::div(1.0, A::mul(F.N, 0.999)), A::div(1.0, A::sub(1.0, 0.999))));
+    } else if (cc < 0.0) {
+        const double cm = 0.0001;
+        cc_phil = A::div(A::mul(cm, F.Mweight), F.Mvolume);
+        ddf = A::mul(0.5, A::add(A::div(1.0, A::mul(F.N, cm)), A::div(1.0, A::sub(1.0, cm))));
+    } else {
+        cc_phil = A::div(A::mul(cc, F.Mweight), F.Mvolume);
+        ddf = A::mul(0.5, A::add(A::div(1.0, A::mul(F.N, cc)), A::div(1.0, A::sub(1.0, cc))));
+    }
+    ddf = A::mul(ddf, kT);
+    double D = A::mul(F.D0, A::div(T, F.Tinit));
+    if (D > F.D0) D = F.D0;
+    const double Dp = A::mul(D, exp(A::mul(-F.gamma, pow(cc_phil, F.nu))));
+    double Mc = A::div(Dp, ddf);
+    if (Mc < 0.000001) Mc = 0.000001;
+    if (Mc > F.D0) Mc = F.D0;
+    if (T <= F.Tcrystal) Mc = A::mul(Mc, 0.001);
+    F.mob[s] = Mc;
+}
+
+// (a[-]*b1 + a[+]*b2 - (b1+b2)*a) / d^2 with b1, b2 the harmonic means of
+// the mobilities toward each neighbour
+__device__ __forceinline__ double fh_axis(double am, double ap, double a0, double bm, double bp, double bo, double coef,
+                                          bool divide)
+{
+    using A = Arith<double>;
+    const double b1 = A::div(2.0, A::add(A::div(1.0, bm), A::div(1.0, bo)));
+    const double b2 = A::div(2.0, A::add(A::div(1.0, bp), A::div(1.0, bo)));
+    const double num = A::sub(A::add(A::mul(am, b1), A::mul(ap, b2)), A::mul(A::add(b1, b2), a0));
+    return divide ? A::div(num, coef) : A::mul(num, coef);
+}
+
+__global__ void fh_update_kernel(JobDev* job)
+{
+    using A = Arith<double>;
+    const JobDev& J = *job;
+    const FhDev& F = *J.fh;
+    const int nx = J.nx, ny = J.ny, nz = J.nz;
+    const size_t n = (size_t)nx * ny * nz;
+    const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (J.step >= J.target || s >= n) return;
+    const int par = (int)(J.step & 1);
+    const double* __restrict__ c = static_cast<const double*>(J.buf[par]);
+    double* __restrict__ out = static_cast<double*>(J.buf[par ^ 1]);
+    const double* __restrict__ mu = F.mu;
+    const double* __restrict__ mob = F.mob;
+    const int x = (int)(s % nx), y = (int)((s / nx) % ny), z = (int)(s / ((size_t)nx * ny));
+    const bool pX = J.flags & JF_PER_X, pY = J.flags & JF_PER_Y, pZ = J.flags & JF_PER_Z;
+    const double a0 = mu[s], bo = mob[s];
+    const int ixm = fh_at(wrap_or_clamp(x - 1, nx, pX), y, z, J), ixp = fh_at(wrap_or_clamp(x + 1, nx, pX), y, z, J);
+    const int izm = fh_at(x, y, wrap_or_clamp(z - 1, nz, pZ), J), izp = fh_at(x, y, wrap_or_clamp(z + 1, nz, pZ), J);
+    const double lx = fh_axis(mu[ixm], mu[ixp], a0, mob[ixm], mob[ixp], bo, J.cx, J.flags & JF_DIV_X);
+    const double lz = fh_axis(mu[izm], mu[izp], a0, mob[izm], mob[izp], bo, J.cz, J.flags & JF_DIV_Z);
+    double lap;
+    if (J.flags & JF_FLAT) {
+        lap = A::add(lx, lz);
+    } else {
+        const int iym = fh_at(x, wrap_or_clamp(y - 1, ny, pY), z, J), iyp = fh_at(x, wrap_or_clamp(y + 1, ny, pY), z, J);
+        const double ly = fh_axis(mu[iym], mu[iyp], a0, mob[iym], mob[iyp], bo, J.cy, J.flags & JF_DIV_Y);
+        lap = A::add(A::add(lx, ly), lz);
+    }
+    out[s] = A::add(c[s], A::mul(J.dtM_dt, lap));  // c += dt * lap (TIPSphil.cpp:194)
+}
+
 // advances the step counter after a generic-path step
 __global__ void ch_step_generic_finish(JobDev* job)
 {

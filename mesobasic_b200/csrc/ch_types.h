@@ -47,6 +47,17 @@ constexpr float kNudge = 1.1920928955078125e-7f;  // 2^-23
 // order).  A strip is the 8 sites x = 4t..4t+3 and nx/2 + 4t..4t+3 of a row.
 constexpr float kMassScale = 4294967296.0f;  // 2^32
 
+// Parameters and work fields of a variable-mobility (TIPSphil) job: the
+// Flory-Huggins chemical potential and Phillies mobility of
+// TIPSphil::updatePhaseField (TIPSphil.cpp:113-211), defaults of its
+// constructor (TIPSphil.cpp:41-59).
+struct FhDev {
+    double alpha, beta, N, A, Tinit, Tbath, Tcrystal, nu, gamma, D0, Mweight, Mvolume;
+    long long nstep;  // Time/nstep: length of the temperature ramp
+    double* mu;       // chemical potential of the step being taken
+    double* mob;      // mobility of the step being taken
+};
+
 // Per-job state in device memory.  The host fills the parameters;
 // `nudge_*`, `mass_last`, `step`, `done` and `err` are updated by the kernels.
 struct alignas(16) JobDev {
@@ -66,6 +77,7 @@ struct alignas(16) JobDev {
     long long nudge_begin;      // first site of the next step's nudge window (JF_MASS)
     long long nudge_count;      // sites in the window; the sign is the nudge's
     double mass_last;           // sum(c) after the last step (JF_MASS)
+    FhDev* fh;                  // variable-mobility model (null: Cahn-Hilliard with constant M)
     double noise;               // per-step noise strength (0: none)
     unsigned long long noise_seed;
     long long noise_step;       // the last step whose noise has been added

@@ -482,7 +482,8 @@ void tune_store(const std::string& key, const mg_tiling& t, double ms)
 // ------------------------------------------------------------------ Job
 size_t Job::device_bytes() const
 {
-    return 2 * g.n * g.es + 4 * sizeof(CUtensorMap) + (size_t)std::max(plan.nitems, 1) * sizeof(long long);
+    return 2 * g.n * g.es + 4 * sizeof(CUtensorMap) + (size_t)std::max(plan.nitems, 1) * sizeof(long long) +
+           (d_fh ? 2 * g.n * sizeof(double) + sizeof(FhDev) : 0);
 }
 
 static void fill_jobdev(const Job& j, JobDev* jd)
@@ -493,6 +494,7 @@ static void fill_jobdev(const Job& j, JobDev* jd)
     jd->buf[1] = j.buf[1];
     jd->tmap = j.d_tmap;
     jd->partial = j.d_partial;
+    jd->fh = j.d_fh;
     jd->nx = g.lnx;
     jd->ny = g.lny;
     jd->nz = g.lnz;
@@ -542,6 +544,9 @@ Engine::~Engine()
         cudaFree(j->buf[1]);
         cudaFree(j->d_tmap);
         cudaFree(j->d_partial);
+        cudaFree(j->d_fh);
+        cudaFree(j->d_mu);
+        cudaFree(j->d_mob);
         delete j;
     }
     jobs.clear();
@@ -585,14 +590,17 @@ int Engine::init(int dev, int capacity)
     return MG_OK;
 }
 
-int Engine::add_job(const mg_ch_params& p, long long target, Job** out)
+int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const mg_fh_params* fh)
 {
     std::unique_ptr<Job> j(new Job);
     j->p = p;
     MG_TRY(make_geometry(p, &j->g));
     if (free_slots_.empty()) return fail(MG_ENOMEM, "no free job slot (capacity %d)", capacity_);
+    if (fh && (p.precision != MG_FP64 || p.mass_correct))
+        return fail(MG_EINVAL, "the variable-mobility model runs in FP64 without mass feedback");
     MG_CUDA(cudaSetDevice(device));
-    j->tiling = batch_tiling ? batch_tiling_for(j->g, info, device) : default_tiling(j->g, info, device);
+    if (fh) j->tiling = mg_tiling{1, 1, 4, 1};  // the per-site path
+    else j->tiling = batch_tiling ? batch_tiling_for(j->g, info, device) : default_tiling(j->g, info, device);
     MG_TRY(plan_tiling(j->g, j->tiling, info, &j->plan));
     if (j->p.mass_correct && !j->plan.tma_ok)
         return fail(MG_EINVAL, "mass_correct needs a shape the tiled kernel takes (nx multiple of %d)", 32);
@@ -602,12 +610,25 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out)
     if (e == cudaSuccess) e = cudaMalloc(&j->buf[1], bytes);
     if (e == cudaSuccess) e = cudaMalloc(&j->d_tmap, 4 * sizeof(CUtensorMap));
     if (e == cudaSuccess) e = cudaMalloc(&j->d_partial, sizeof(long long) * std::max(j->plan.nitems, 1));
+    if (fh) {
+        if (e == cudaSuccess) e = cudaMalloc(&j->d_fh, sizeof(FhDev));
+        if (e == cudaSuccess) e = cudaMalloc(&j->d_mu, j->g.n * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&j->d_mob, j->g.n * sizeof(double));
+        if (e == cudaSuccess) {
+            const FhDev f{fh->alpha, fh->beta, fh->N, fh->A, fh->Tinit, fh->Tbath, fh->Tcrystal, fh->nu, fh->gamma,
+                          fh->D0, fh->Mweight, fh->Mvolume, fh->nstep, j->d_mu, j->d_mob};
+            e = cudaMemcpy(j->d_fh, &f, sizeof f, cudaMemcpyHostToDevice);
+        }
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         cudaFree(j->buf[0]);
         cudaFree(j->buf[1]);
         cudaFree(j->d_tmap);
         cudaFree(j->d_partial);
+        cudaFree(j->d_fh);
+        cudaFree(j->d_mu);
+        cudaFree(j->d_mob);
         return fail(e == cudaErrorMemoryAllocation ? MG_ENOMEM : MG_ECUDA, "allocating %zu bytes: %s", 2 * bytes,
                     cudaGetErrorString(e));
     }
@@ -644,7 +665,8 @@ void Engine::remove_job(Job* j)
     jobs.erase(it);
     // freed at the next rebuild (which waits for the stream anyway) or at
     // destruction: cudaFree waits for the whole device, once per call
-    graveyard_.insert(graveyard_.end(), {j->buf[0], j->buf[1], (void*)j->d_tmap, (void*)j->d_partial});
+    graveyard_.insert(graveyard_.end(), {j->buf[0], j->buf[1], (void*)j->d_tmap, (void*)j->d_partial, (void*)j->d_fh,
+                                         (void*)j->d_mu, (void*)j->d_mob});
     free_slots_.push_back(j->slot);
     delete j;
     dirty_ = true;
@@ -652,6 +674,7 @@ void Engine::remove_job(Job* j)
 
 int Engine::set_tiling(Job* j, const mg_tiling& t)
 {
+    if (j->d_fh && t.path != 1) return fail(MG_EINVAL, "the variable-mobility model runs on the per-site path (path 1)");
     TilePlan pl;
     MG_TRY(plan_tiling(j->g, t, info, &pl));
     if (j->p.mass_correct && !pl.tma_ok) return fail(MG_EINVAL, "mass_correct needs the tiled kernel");
@@ -864,8 +887,14 @@ int Engine::launch_lane(const Group& g, Job* generic_job, cudaStream_t st)
     if (g.generic) {
         Job* j = generic_job;
         const unsigned blocks = (unsigned)((j->g.n + 255) / 256);
-        if (g.fp32) ch_step_generic_kernel<float><<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
-        else ch_step_generic_kernel<double><<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
+        if (j->d_fh) {  // variable mobility: mu and mobility, then the update
+            fh_mu_mob_kernel<<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
+            fh_update_kernel<<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
+        } else if (g.fp32) {
+            ch_step_generic_kernel<float><<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
+        } else {
+            ch_step_generic_kernel<double><<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
+        }
         ch_step_generic_finish<<<1, 32, 0, st>>>(d_jobs_ + j->slot);
     } else {
         StepArgs a;
@@ -1076,6 +1105,15 @@ int Engine::download(Job* j, double* host)
         MG_CUDA(cudaMemcpyAsync(host, d_stage_, j->g.n * 8, cudaMemcpyDeviceToHost, stream));
     }
     MG_CUDA(cudaStreamSynchronize(stream));
+    return MG_OK;
+}
+
+int Engine::mobility(Job* j, double* host)
+{
+    if (!host) return fail(MG_EINVAL, "null field");
+    if (!j->d_fh) return fail(MG_EINVAL, "not a variable-mobility job");
+    MG_TRY(sync(-1));
+    MG_CUDA(cudaMemcpy(host, j->d_mob, j->g.n * sizeof(double), cudaMemcpyDeviceToHost));
     return MG_OK;
 }
 

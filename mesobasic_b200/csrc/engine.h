@@ -78,6 +78,9 @@ struct Job {
     void* buf[2] = {nullptr, nullptr};
     CUtensorMap* d_tmap = nullptr;  // 4 maps
     long long* d_partial = nullptr;
+    FhDev* d_fh = nullptr;        // variable-mobility model (mg_fh_create)
+    double* d_mu = nullptr;       // its chemical potential ...
+    double* d_mob = nullptr;      // ... and mobility fields
     int slot = -1;
     long long target = -1;  // device step target (-1: unbounded)
     size_t device_bytes() const;
@@ -90,7 +93,8 @@ class Engine {
     int init(int device, int capacity);
 
     // job lifetime: allocate buffers + maps, take a slot
-    int add_job(const mg_ch_params& p, long long target, Job** out);
+    int add_job(const mg_ch_params& p, long long target, Job** out, const mg_fh_params* fh = nullptr);
+    int mobility(Job* j, double* host);  // last step's mobility (variable-mobility jobs)
     void remove_job(Job* j);  // releases the job; its device memory is freed at the next rebuild
     int set_tiling(Job* j, const mg_tiling& t);
 

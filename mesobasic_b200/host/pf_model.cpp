@@ -4,14 +4,17 @@
 #include <stdexcept>
 
 #include "chbasic_gpu.hpp"
+#include "tipsphil_gpu.hpp"
 
 PFBaseClass* PFBaseClass::PFFactory(const CommonParams& p, const InputFile& in)
 {
     // PFBaseClass.cpp:33: the type defaults to "CHBasic"
     const std::string type = in("PFApp/type", "CHBasic");
     if (type == "CHBasic" || type == "CHBasicGPU") return new CHBasicGPU(p, in);
+    if (type == "TIPSphil" || type == "TIPSphilGPU") return new TIPSphilGPU(p, in);
     throw std::invalid_argument("PFApp/type '" + type +
-                                "' is not provided by this build (available: CHBasic, CHBasicGPU)");
+                                "' is not provided by this build (available: CHBasic, CHBasicGPU, TIPSphil, "
+                                "TIPSphilGPU)");
 }
 
 PFApp::PFApp(const InputFile& in)

@@ -38,7 +38,8 @@ struct CommonParams {
 
 class PFBaseClass {
 public:
-    // "CHBasic" and "CHBasicGPU": the GPU Cahn-Hilliard model
+    // "CHBasic"/"CHBasicGPU": the GPU Cahn-Hilliard model; "TIPSphil"/
+    // "TIPSphilGPU": the variable-mobility Flory-Huggins model
     static PFBaseClass* PFFactory(const CommonParams&, const InputFile&);
 
     virtual void initPhaseField() = 0;

@@ -84,6 +84,9 @@ def ref_lib():
         _ref.chref_run.restype = ctypes.c_int
         _ref.chref_ic.argtypes = [_i3, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_uint32, _dp]
         _ref.chref_ic.restype = ctypes.c_int
+        _ref.fhref_run.argtypes = [_i3, _d3, ctypes.c_double, _i3, _dp, ctypes.c_int, ctypes.c_int, _dp,
+                                   ctypes.c_int, _dp]
+        _ref.fhref_run.restype = ctypes.c_int
     return _ref
 
 
@@ -143,6 +146,25 @@ def ref_run(c, dims, spacing=(1.0, 1.0, 1.0), dt=0.01, M=1.0, kap=1.0, nsteps=1,
     a = _as_field(c, dims)
     out = np.empty_like(a)
     ref_lib().chref_run(_i3(*dims), _d3(*spacing), dt, M, kap, _i3(*bc), _ptr(a), nsteps, _ptr(out))
+    return out
+
+
+# TIPSphil's parameters in the order fhref_run takes them, with the
+# reference constructor's defaults (TIPSphil.cpp:41-59)
+FH_KEYS = ("alpha", "beta", "N", "A", "Tinit", "Tbath", "Tcrystal", "nu", "gamma", "D0", "Mweight", "Mvolume", "kap")
+FH_DEFAULTS = dict(alpha=1.0, beta=1.0, N=100.0, A=1.0, Tinit=273.0, Tbath=273.0, Tcrystal=273.0, nu=1.0,
+                   gamma=10.0, D0=1e-7, Mweight=100.0, Mvolume=0.1, kap=1.0)
+
+
+def fh_ref_run(c, dims, fh, nstep_total, first, nsteps, spacing=(1.0, 1.0, 1.0), dt=0.01, bc=(1, 1, 1)):
+    """Steps first..first+nsteps-1 of the reference's own TIPSphil update
+    (Flory-Huggins mu, Phillies mobility, variable-mobility Laplacian) on c,
+    noise off; fh maps FH_KEYS to values (missing keys: FH_DEFAULTS)."""
+    a = _as_field(c, dims)
+    out = np.empty_like(a)
+    prm = np.array([fh.get(k, FH_DEFAULTS[k]) for k in FH_KEYS], dtype=np.float64)
+    ref_lib().fhref_run(_i3(*dims), _d3(*spacing), dt, _i3(*bc), _ptr(prm), nstep_total, first, _ptr(a), nsteps,
+                        _ptr(out))
     return out
 
 

@@ -72,8 +72,8 @@ def run_driver(tmp_path, text, *args, timeout=300):
 
 
 def test_unknown_model_type_fails_loudly(tmp_path):
-    r = run_driver(tmp_path, "[Domain]\nnx=8\n[]\n[PFApp]\napp = true\ntype = TIPSphil\n[]\n")
-    assert r.returncode == 1 and "TIPSphil" in r.stderr
+    r = run_driver(tmp_path, "[Domain]\nnx=8\n[]\n[PFApp]\napp = true\ntype = SIPS\n[]\n")
+    assert r.returncode == 1 and "SIPS" in r.stderr
 
 
 def test_more_outputs_than_steps_is_an_error(tmp_path):

@@ -1,0 +1,109 @@
+"""The variable-mobility (TIPSphil) step against the reference's own
+TIPSphil::updatePhaseField run on the same field (oracle.fh_ref_run, noise
+off).  FP64; log, exp and pow differ from the host's libm by an ulp or two,
+so the bar is a relative max-norm of 1e-12 rather than bit identity."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import mesobasic_b200 as mb
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+# a quench that phase-separates: chi = alpha/T + beta crosses the spinodal
+QUENCH = dict(alpha=150.0, beta=0.1, N=50.0, A=1.0, Tinit=300.0, Tbath=280.0, Tcrystal=200.0, nu=1.0,
+              gamma=1.0, D0=1.0, Mweight=0.5, Mvolume=1.0)
+
+
+def gpu_run(dims, fh, nstep_total, ic, nsteps, dt=0.01, kap=1.0, spacing=(1.0, 1.0, 1.0), bc=(1, 1, 1)):
+    p = mb.make_params(*dims, dt, kappa=kap, dx=spacing[0], dy=spacing[1], dz=spacing[2], bc=bc)
+    with mb.CHSim(p, fh=mb.make_fh_params(nstep_total, **fh)) as sim:
+        sim.set_field(ic)
+        sim.step(nsteps)
+        return sim.get_field(), sim.mobility()
+
+
+def rel_err(got, want):
+    return np.abs(got - want).max() / np.abs(want).max()
+
+
+CASES = [
+    ("3d periodic", (24, 20, 16), QUENCH, (1.0, 1.0, 1.0), (1, 1, 1), 0.3, 0.1),
+    ("3d no-flux, unequal spacing", (20, 12, 10), QUENCH, (1.0, 1.25, 1.5), (0, 0, 1), 0.35, 0.1),
+    ("2d mixed boundaries", (48, 36, 1), QUENCH, (1.0, 1.0, 1.0), (1, 0, 1), 0.3, 0.1),
+    # values below 0 (the sqrt branch of mu, the lower-limit mobility), the
+    # crystallisation factor (T <= Tcrystal) and the D0 clamps
+    ("branches", (16, 16, 8), dict(QUENCH, Tcrystal=290.0, D0=0.5), (1.0, 1.0, 1.0), (1, 1, 1), 0.02, 0.1),
+]
+
+
+@pytest.mark.parametrize("name,dims,fh,spacing,bc,co,amp", CASES, ids=[c[0] for c in CASES])
+def test_matches_reference_tipsphil(oracle, name, dims, fh, spacing, bc, co, amp):
+    ic = oracle.ic(dims, co, amp, False, 21)
+    want = oracle.fh_ref_run(ic, dims, dict(fh, kap=1.0), 50, 1, 10, spacing=spacing, dt=0.01, bc=bc)
+    got, mob = gpu_run(dims, fh, 50, ic, 10, spacing=spacing, bc=bc)
+    assert rel_err(got, want) <= 1e-12, rel_err(got, want)
+    assert np.all(mob > 0) and np.all(mob <= fh["D0"])
+    assert np.abs(got - ic).max() > 1e-4  # the model moved the field
+
+
+def test_reference_defaults_run(oracle):
+    """The reference's defaults (D0 = 1e-7: the mobility sits at its clamps)."""
+    dims = (16, 12, 8)
+    ic = oracle.ic(dims, 0.5, 0.1, False, 2)
+    want = oracle.fh_ref_run(ic, dims, {}, 20, 1, 5)
+    got, mob = gpu_run(dims, {}, 20, ic, 5)
+    assert rel_err(got, want) <= 1e-12
+    assert np.allclose(mob, 1e-7 * 0.001, rtol=0, atol=1e-20) or np.allclose(mob, 1e-7, rtol=1e-15)
+
+
+def test_rejects_fp32_and_bad_parameters():
+    with pytest.raises(mb.MGError):
+        mb.CHSim(mb.make_params(16, 8, 8, 0.01, precision="fp32"), fh=mb.make_fh_params(10))
+    with pytest.raises(mb.MGError):
+        mb.CHSim(mb.make_params(16, 8, 8, 0.01), fh=mb.make_fh_params(0))
+
+
+def test_driver_runs_tipsphil(tmp_path):
+    text = """[Domain]
+nx = 32
+ny = 24
+nz = 16
+[]
+[Time]
+nstep = 40
+dt = 0.01
+[]
+[Output]
+numOutputs = 2
+[]
+[PFApp]
+app = true
+type = TIPSphil
+co = 0.3
+alpha = 150
+beta = 0.1
+N = 50
+Tinit = 300
+Tbath = 280
+Tcrystal = 200
+gamma = 1
+D0 = 1
+Mweight = 0.5
+Mvolume = 1
+mobStep = 10
+noiseStr = 0.05
+[]
+"""
+    (tmp_path / "input.dat").write_text(text)
+    r = subprocess.run([os.path.join(ROOT, "mesobasic_b200", "meso_b200")], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    names = sorted(os.listdir(tmp_path / "vtkoutput"))
+    assert names == ["c_0.vtk", "c_20.vtk", "c_40.vtk", "mob_10.vtk"], names
+    body = (tmp_path / "vtkoutput" / "mob_10.vtk").read_text().splitlines()
+    assert body[10] == "SCALARS mob float" and len(body) == 12 + 32 * 24 * 16
