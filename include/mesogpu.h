@@ -165,6 +165,10 @@ typedef struct {
     double D0;              /* diffusivity and mobility cap [PFApp/D0 (1e-7)] */
     double Mweight, Mvolume;/* phi -> g/L [PFApp/Mweight (100), Mvolume (0.1)] */
     long long nstep;        /* steps of the quench [Time/nstep] */
+    int bath;               /* 0: uniform ramp (TIPSphil); 1: the 1-D bath profile of
+                               TIPSbathPHIL, T = (Tinit-Tbath)*erf(i/(2*sqrt(thermCond*step*dt)))
+                               + Tbath with i the 1-based x index (TIPSbathPHIL.cpp:118-121) */
+    double thermCond;       /* [PFApp/thermCond (1)] */
 } mg_fh_params;
 
 /* A simulation stepped by the variable-mobility update of

@@ -52,14 +52,15 @@ FH_DEFAULTS = dict(alpha=1.0, beta=1.0, N=100.0, A=1.0, Tinit=273.0, Tbath=273.0
                    gamma=10.0, D0=1e-7, Mweight=100.0, Mvolume=0.1)
 
 
-def make_fh_params(nstep, **kw) -> FhParams:
-    """Variable-mobility (TIPSphil) parameters; unnamed ones take the
+def make_fh_params(nstep, bath=False, thermCond=1.0, **kw) -> FhParams:
+    """Variable-mobility parameters: TIPSphil's uniform quench, or with
+    bath=True TIPSbathPHIL's 1-D bath profile; unnamed ones take the
     reference's defaults."""
     unknown = set(kw) - set(FH_DEFAULTS)
     if unknown:
         raise ValueError(f"unknown variable-mobility parameters {sorted(unknown)}")
     v = dict(FH_DEFAULTS, **kw)
-    return FhParams(*(float(v[k]) for k in FH_DEFAULTS), int(nstep))
+    return FhParams(*(float(v[k]) for k in FH_DEFAULTS), int(nstep), int(bool(bath)), float(thermCond))
 
 
 class CHSim:

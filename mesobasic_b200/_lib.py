@@ -44,7 +44,8 @@ class FhParams(ctypes.Structure):
     _fields_ = [("alpha", ctypes.c_double), ("beta", ctypes.c_double), ("N", ctypes.c_double), ("A", ctypes.c_double),
                 ("Tinit", ctypes.c_double), ("Tbath", ctypes.c_double), ("Tcrystal", ctypes.c_double),
                 ("nu", ctypes.c_double), ("gamma", ctypes.c_double), ("D0", ctypes.c_double),
-                ("Mweight", ctypes.c_double), ("Mvolume", ctypes.c_double), ("nstep", ctypes.c_longlong)]
+                ("Mweight", ctypes.c_double), ("Mvolume", ctypes.c_double), ("nstep", ctypes.c_longlong),
+                ("bath", ctypes.c_int), ("thermCond", ctypes.c_double)]
 
 
 class Stats(ctypes.Structure):

@@ -54,6 +54,8 @@ int mg_fh_create(const mg_ch_params* params, const mg_fh_params* fh, int device,
     for (double x : v)
         if (!std::isfinite(x)) return fail(MG_EINVAL, "variable-mobility parameters must be finite");
     if (fh->nstep < 1) return fail(MG_EINVAL, "nstep must be >= 1");
+    if (fh->bath != 0 && fh->bath != 1) return fail(MG_EINVAL, "bath must be 0 or 1");
+    if (!std::isfinite(fh->thermCond)) return fail(MG_EINVAL, "thermCond must be finite");
     if (fh->N == 0 || fh->Mvolume == 0 || fh->Tinit == 0) return fail(MG_EINVAL, "N, Mvolume and Tinit must be nonzero");
     mg::Geometry g;
     MG_TRY(mg::make_geometry(*params, &g));

@@ -894,12 +894,19 @@ __global__ void fh_mu_mob_kernel(JobDev* job)
     const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (J.step >= J.target || s >= n) return;
     const double* __restrict__ c = static_cast<const double*>(J.buf[J.step & 1]);
-    // temperature of the step being taken (PFApp passes it as current_step)
+    // temperature of the step being taken (PFApp passes it as current_step):
+    // a uniform ramp, or the bath profile along x (TIPSbathPHIL.cpp:118-121)
     const double cs = (double)(J.step + 1);
-    const double T = A::sub(F.Tinit, A::mul(A::sub(F.Tinit, F.Tbath), A::div(cs, (double)F.nstep)));
+    const int x = (int)(s % nx), y = (int)((s / nx) % ny), z = (int)(s / ((size_t)nx * ny));
+    double T;
+    if (F.bath)
+        T = A::add(A::mul(A::sub(F.Tinit, F.Tbath),
+                          erf(A::div((double)(x + 1), A::mul(2.0, sqrt(A::mul(A::mul(F.thermCond, cs), J.dtM_dt)))))),
+                   F.Tbath);
+    else
+        T = A::sub(F.Tinit, A::mul(A::sub(F.Tinit, F.Tbath), A::div(cs, (double)F.nstep)));
     const double kT = A::div(T, 273.0);
     const double chi = A::add(A::div(F.alpha, T), F.beta);
-    const int x = (int)(s % nx), y = (int)((s / nx) % ny), z = (int)(s / ((size_t)nx * ny));
     const bool pX = J.flags & JF_PER_X, pY = J.flags & JF_PER_Y, pZ = J.flags & JF_PER_Z;
     const double cc = c[s];
     const double xp = c[fh_at(wrap_or_clamp(x + 1, nx, pX), y, z, J)], xm = c[fh_at(wrap_or_clamp(x - 1, nx, pX), y, z, J)];

@@ -54,6 +54,8 @@ constexpr float kMassScale = 4294967296.0f;  // 2^32
 struct FhDev {
     double alpha, beta, N, A, Tinit, Tbath, Tcrystal, nu, gamma, D0, Mweight, Mvolume;
     long long nstep;  // Time/nstep: length of the temperature ramp
+    int bath;         // 1: temperature from the bath profile (TIPSbathPHIL)
+    double thermCond;
     double* mu;       // chemical potential of the step being taken
     double* mob;      // mobility of the step being taken
 };

@@ -616,7 +616,7 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const mg
         if (e == cudaSuccess) e = cudaMalloc(&j->d_mob, j->g.n * sizeof(double));
         if (e == cudaSuccess) {
             const FhDev f{fh->alpha, fh->beta, fh->N, fh->A, fh->Tinit, fh->Tbath, fh->Tcrystal, fh->nu, fh->gamma,
-                          fh->D0, fh->Mweight, fh->Mvolume, fh->nstep, j->d_mu, j->d_mob};
+                          fh->D0, fh->Mweight, fh->Mvolume, fh->nstep, fh->bath, fh->thermCond, j->d_mu, j->d_mob};
             e = cudaMemcpy(j->d_fh, &f, sizeof f, cudaMemcpyHostToDevice);
         }
     }

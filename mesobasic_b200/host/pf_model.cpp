@@ -12,9 +12,10 @@ PFBaseClass* PFBaseClass::PFFactory(const CommonParams& p, const InputFile& in)
     const std::string type = in("PFApp/type", "CHBasic");
     if (type == "CHBasic" || type == "CHBasicGPU") return new CHBasicGPU(p, in);
     if (type == "TIPSphil" || type == "TIPSphilGPU") return new TIPSphilGPU(p, in);
+    if (type == "TIPSbathPHIL" || type == "TIPSbathPHILGPU") return new TIPSphilGPU(p, in, true);
     throw std::invalid_argument("PFApp/type '" + type +
                                 "' is not provided by this build (available: CHBasic, CHBasicGPU, TIPSphil, "
-                                "TIPSphilGPU)");
+                                "TIPSphilGPU, TIPSbathPHIL, TIPSbathPHILGPU)");
 }
 
 PFApp::PFApp(const InputFile& in)

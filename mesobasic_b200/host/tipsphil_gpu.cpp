@@ -1,6 +1,7 @@
 // See tipsphil_gpu.hpp.
 #include "tipsphil_gpu.hpp"
 
+#include <cmath>
 #include <cstdio>
 #include <stdexcept>
 #include <string>
@@ -17,7 +18,7 @@ constexpr int kMaxPending = 1000;
 
 }  // namespace
 
-TIPSphilGPU::TIPSphilGPU(const CommonParams& pin, const InputFile& in) : p(pin)
+TIPSphilGPU::TIPSphilGPU(const CommonParams& pin, const InputFile& in, bool bath_) : p(pin), bath(bath_)
 {
     if (p.np != 1) throw std::invalid_argument("TIPSphilGPU runs one simulation per process (np must be 1)");
     gp.nx = p.NX;
@@ -29,7 +30,7 @@ TIPSphilGPU::TIPSphilGPU(const CommonParams& pin, const InputFile& in) : p(pin)
     gp.dt = p.dt;
     gp.M = in("PFApp/M", 1.0);
     gp.kappa = in("PFApp/kap", 1.0);
-    gp.bx = in("PFApp/bx", 1);
+    gp.bx = in("PFApp/bx", bath ? 0 : 1);  // TIPSbathPHIL.cpp:18: no-flux x by default
     gp.by = in("PFApp/by", 1);
     gp.bz = in("PFApp/bz", 1);
     gp.precision = MG_FP64;
@@ -37,7 +38,7 @@ TIPSphilGPU::TIPSphilGPU(const CommonParams& pin, const InputFile& in) : p(pin)
     gp.noise = in("PFApp/noiseStr", 0.1);
     seed = (unsigned)in("PFApp/seed", 42);
     gp.noise_seed = (unsigned long long)in("PFApp/noise_seed", (int)seed);
-    mobStep = in("PFApp/mobStep", 1);
+    mobStep = bath ? -1 : in("PFApp/mobStep", 1);  // TIPSbathPHIL writes no mobility
     co = in("PFApp/co", 0.5);
     fp.alpha = in("PFApp/alpha", 1.0);
     fp.beta = in("PFApp/beta", 1.0);
@@ -52,6 +53,8 @@ TIPSphilGPU::TIPSphilGPU(const CommonParams& pin, const InputFile& in) : p(pin)
     fp.Mweight = in("PFApp/Mweight", 100.0);
     fp.Mvolume = in("PFApp/Mvolume", 0.1);
     fp.nstep = p.nstep;
+    fp.bath = bath ? 1 : 0;
+    fp.thermCond = in("PFApp/thermCond", 1.0);
     check(mg_fh_create(&gp, &fp, in("PFApp/device", 0), &h), "mg_fh_create");
 }
 
@@ -105,6 +108,20 @@ void TIPSphilGPU::outputPhaseField()
 {
     flush();
     char path[64];
-    std::snprintf(path, sizeof path, "vtkoutput/c_%d.vtk", current_step);
-    check(mg_ch_write_vtk(h, path, "c", p.iskip, p.jskip, p.kskip), "mg_ch_write_vtk");
+    std::snprintf(path, sizeof path, "vtkoutput/%s_%d.vtk", bath ? "polymer" : "c", current_step);
+    check(mg_ch_write_vtk(h, path, bath ? "polymer" : "c", p.iskip, p.jskip, p.kskip), "mg_ch_write_vtk");
+    if (bath) {
+        // TIPSbathPHIL's TempOut: 460 from the initializer, then the bath
+        // profile of the last step (TIPSbathPHIL.cpp:118-125)
+        std::vector<double> T((size_t)gp.nx * gp.ny * gp.nz);
+        for (size_t s = 0; s < T.size(); ++s) {
+            const int i = (int)(s % gp.nx) + 1;
+            T[s] = current_step == 0 ? 460.0
+                                     : (fp.Tinit - fp.Tbath) * std::erf(i / (2.0 * std::sqrt(fp.thermCond * double(current_step) * gp.dt))) +
+                                           fp.Tbath;
+        }
+        std::snprintf(path, sizeof path, "vtkoutput/temp_%d.vtk", current_step);
+        const int dims[3] = {gp.nx, gp.ny, gp.nz};
+        check(mg_vtk_write(path, "temp", T.data(), dims, p.iskip, p.jskip, p.kskip), "mg_vtk_write");
+    }
 }

@@ -12,6 +12,11 @@
 // PFApp/noise_seed, default seed) where the reference seeds rand() from the
 // clock.  Output: c as legacy VTK at every output step; the mobility as
 // vtkoutput/mob_<mobStep>.vtk after step mobStep, as the reference writes it.
+//
+// With `bath` the model is TIPSbathPHIL (TIPSbathPHIL.cpp): the temperature
+// is the 1-D bath profile along x (key thermCond, default 1), bx defaults to
+// 0, and each output writes polymer_<step>.vtk (c) and temp_<step>.vtk (the
+// temperature: 460 at step 0, the profile of the last step after it).
 #pragma once
 
 #include "mesogpu.h"
@@ -19,7 +24,7 @@
 
 class TIPSphilGPU : public PFBaseClass {
 public:
-    TIPSphilGPU(const CommonParams& p, const InputFile& in);
+    TIPSphilGPU(const CommonParams& p, const InputFile& in, bool bath = false);
     ~TIPSphilGPU() override;
 
     void initPhaseField() override;
@@ -37,6 +42,7 @@ private:
     int current_step = 0;
     int pending = 0;
     int mobStep;
+    bool bath;
     double co;
     unsigned seed;
 };

@@ -84,8 +84,8 @@ def ref_lib():
         _ref.chref_run.restype = ctypes.c_int
         _ref.chref_ic.argtypes = [_i3, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_uint32, _dp]
         _ref.chref_ic.restype = ctypes.c_int
-        _ref.fhref_run.argtypes = [_i3, _d3, ctypes.c_double, _i3, _dp, ctypes.c_int, ctypes.c_int, _dp,
-                                   ctypes.c_int, _dp]
+        _ref.fhref_run.argtypes = [_i3, _d3, ctypes.c_double, _i3, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                   ctypes.c_int, _dp, ctypes.c_int, _dp]
         _ref.fhref_run.restype = ctypes.c_int
     return _ref
 
@@ -156,15 +156,17 @@ FH_DEFAULTS = dict(alpha=1.0, beta=1.0, N=100.0, A=1.0, Tinit=273.0, Tbath=273.0
                    gamma=10.0, D0=1e-7, Mweight=100.0, Mvolume=0.1, kap=1.0)
 
 
-def fh_ref_run(c, dims, fh, nstep_total, first, nsteps, spacing=(1.0, 1.0, 1.0), dt=0.01, bc=(1, 1, 1)):
+def fh_ref_run(c, dims, fh, nstep_total, first, nsteps, spacing=(1.0, 1.0, 1.0), dt=0.01, bc=(1, 1, 1), bath=False,
+               thermCond=1.0):
     """Steps first..first+nsteps-1 of the reference's own TIPSphil update
-    (Flory-Huggins mu, Phillies mobility, variable-mobility Laplacian) on c,
-    noise off; fh maps FH_KEYS to values (missing keys: FH_DEFAULTS)."""
+    (or TIPSbathPHIL's with bath=True: Flory-Huggins mu, Phillies mobility,
+    variable-mobility Laplacian) on c, noise off; fh maps FH_KEYS to values
+    (missing keys: FH_DEFAULTS)."""
     a = _as_field(c, dims)
     out = np.empty_like(a)
     prm = np.array([fh.get(k, FH_DEFAULTS[k]) for k in FH_KEYS], dtype=np.float64)
-    ref_lib().fhref_run(_i3(*dims), _d3(*spacing), dt, _i3(*bc), _ptr(prm), nstep_total, first, _ptr(a), nsteps,
-                        _ptr(out))
+    ref_lib().fhref_run(_i3(*dims), _d3(*spacing), dt, _i3(*bc), _ptr(prm), int(bool(bath)), float(thermCond),
+                        nstep_total, first, _ptr(a), nsteps, _ptr(out))
     return out
 
 

@@ -107,3 +107,63 @@ noiseStr = 0.05
     assert names == ["c_0.vtk", "c_20.vtk", "c_40.vtk", "mob_10.vtk"], names
     body = (tmp_path / "vtkoutput" / "mob_10.vtk").read_text().splitlines()
     assert body[10] == "SCALARS mob float" and len(body) == 12 + 32 * 24 * 16
+
+
+@pytest.mark.parametrize("thermCond,dims", [(1.0, (32, 12, 8)), (4.0, (40, 24, 1))])
+def test_bath_matches_reference_tipsbathphil(oracle, thermCond, dims):
+    """TIPSbathPHIL: the temperature follows the 1-D bath profile along x."""
+    fh = dict(QUENCH, Tinit=320.0, Tbath=260.0)
+    ic = oracle.ic(dims, 0.3, 0.1, False, 8)
+    want = oracle.fh_ref_run(ic, dims, dict(fh, kap=1.0), 50, 1, 10, bc=(0, 1, 1), bath=True, thermCond=thermCond)
+    p = mb.make_params(*dims, 0.01, bc=(0, 1, 1))
+    with mb.CHSim(p, fh=mb.make_fh_params(50, bath=True, thermCond=thermCond, **fh)) as sim:
+        sim.set_field(ic)
+        sim.step(10)
+        got = sim.get_field()
+    assert rel_err(got, want) <= 1e-12, rel_err(got, want)
+    # and not the uniform ramp
+    ramp = oracle.fh_ref_run(ic, dims, dict(fh, kap=1.0), 50, 1, 10, bc=(0, 1, 1))
+    assert np.abs(got - ramp).max() > 1e-6
+
+
+def test_driver_runs_tipsbathphil(tmp_path):
+    text = """[Domain]
+nx = 32
+ny = 16
+nz = 8
+[]
+[Time]
+nstep = 20
+dt = 0.01
+[]
+[Output]
+numOutputs = 1
+[]
+[PFApp]
+app = true
+type = TIPSbathPHIL
+co = 0.3
+alpha = 150
+beta = 0.1
+N = 50
+Tinit = 320
+Tbath = 260
+Tcrystal = 200
+gamma = 1
+D0 = 1
+Mweight = 0.5
+Mvolume = 1
+thermCond = 2
+noiseStr = 0
+[]
+"""
+    (tmp_path / "input.dat").write_text(text)
+    r = subprocess.run([os.path.join(ROOT, "mesobasic_b200", "meso_b200")], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    names = sorted(os.listdir(tmp_path / "vtkoutput"))
+    assert names == ["polymer_0.vtk", "polymer_20.vtk", "temp_0.vtk", "temp_20.vtk"], names
+    t0 = (tmp_path / "vtkoutput" / "temp_0.vtk").read_text().splitlines()
+    assert t0[12] == "460.000"
+    t20 = [float(v) for v in (tmp_path / "vtkoutput" / "temp_20.vtk").read_text().splitlines()[12:12 + 32]]
+    assert 260.0 < t20[0] < t20[-1] <= 320.0  # warmer away from the bath at x = 0
