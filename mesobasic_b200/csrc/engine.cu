@@ -163,9 +163,22 @@ bool tma_shape_ok(const Geometry& g)
 static int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
 // the step kernel has a compile-time row-width variant for this job
+// row widths with compile-time variants of the step kernel: 256 with ring
+// depths 4 and 8; the widths of batched and large jobs with depth 4
+static const int kFixedWidths[] = {64, 96, 128, 160, 192, 224, 256, 512};
+
+static bool fixed_width(int nx, int nbuf)
+{
+    if (nx == 256) return nbuf == 4 || nbuf == 8;
+    if (nbuf != 4) return false;
+    for (int w : kFixedWidths)
+        if (w == nx) return true;
+    return false;
+}
+
 bool fixed_width_kernel(const Geometry& g, int nbuf)
 {
-    return geometry_simple(g) && !g.flat && (nbuf == 4 || nbuf == 8) && g.lnx == 256;
+    return geometry_simple(g) && !g.flat && fixed_width(g.lnx, nbuf);
 }
 
 int plan_tiling(const Geometry& g, const mg_tiling& t, const DevInfo& d, TilePlan* out)
@@ -235,7 +248,17 @@ template <typename T, bool FLAT, bool MASS>
 static StepKernel pick_fixed(int nx, int nbuf)
 {
     if (nx == 256) return nbuf == 8 ? ch_step_kernel<T, 8, FLAT, true, MASS, 256> : ch_step_kernel<T, 4, FLAT, true, MASS, 256>;
-    return nullptr;
+    if (nbuf != 4) return nullptr;
+    switch (nx) {
+    case 64: return ch_step_kernel<T, 4, FLAT, true, MASS, 64>;
+    case 96: return ch_step_kernel<T, 4, FLAT, true, MASS, 96>;
+    case 128: return ch_step_kernel<T, 4, FLAT, true, MASS, 128>;
+    case 160: return ch_step_kernel<T, 4, FLAT, true, MASS, 160>;
+    case 192: return ch_step_kernel<T, 4, FLAT, true, MASS, 192>;
+    case 224: return ch_step_kernel<T, 4, FLAT, true, MASS, 224>;
+    case 512: return ch_step_kernel<T, 4, FLAT, true, MASS, 512>;
+    default: return nullptr;
+    }
 }
 
 template <typename T, bool MASS>
@@ -272,10 +295,10 @@ int prepare_kernels(const DevInfo& d)
                 for (int nb : nbufs)
                     for (int bl : {256, 512})
                         for (int ms = 0; ms < 2; ++ms)
-                            for (int fx : {0, 256})
-                            MG_CUDA(cudaFuncSetAttribute(step_kernel(f32, fl, nb, sm, bl, ms && f32, fx),
-                                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                         (int)d.smem_optin));
+                            for (int fx : {0, 64, 96, 128, 160, 192, 224, 256, 512})
+                                MG_CUDA(cudaFuncSetAttribute(step_kernel(f32, fl, nb, sm, bl, ms && f32, fx),
+                                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                             (int)d.smem_optin));
     done = true;
     return MG_OK;
 }

@@ -259,3 +259,12 @@ def test_fixed_width_fp32_within_tolerance(oracle, mc):
     for t in [(6, 3, 4, 0), (5, 2, 8, 0)]:
         got = run_gpu(mb.make_params(*dims, 0.005, kappa=1.5, precision="fp32", mass_correct=mc), ic, 100, tiling=t)
         assert np.abs(got - want).max() <= 1e-4, (t, np.abs(got - want).max())
+
+
+@pytest.mark.parametrize("dims,tiling", [((64, 20, 9), (6, 2, 4, 0)), ((96, 18, 23), (7, 3, 4, 0)),
+                                         ((160, 10, 12), (4, 2, 4, 0)), ((512, 6, 7), (2, 2, 4, 0))])
+def test_other_fixed_widths_fp64_bit_identical_to_oracle(oracle, dims, tiling):
+    ic = oracle.ic(dims, -0.1, 0.4, False, 23)
+    want = oracle.run(ic, dims, (1.0, 1.0, 1.0), 0.005, 1.0, 0.9, 5)
+    got = run_gpu(mb.make_params(*dims, 0.005, kappa=0.9), ic, 5, tiling=tiling)
+    assert np.array_equal(got, want), np.abs(got - want).max()
