@@ -265,6 +265,8 @@ int mg_batch_create(const mg_ch_params* jobs, int njobs, int device, mg_batch_t*
     if (!b) return fail(MG_ENOMEM, "host allocation failed");
     MG_TRY(b->eng.init(device, njobs));
     b->eng.batch_tiling = true;
+    b->eng.batch_threads = mg::mg_env_int("MG_BATCH_THREADS", 320);
+    b->eng.batch_planes = mg::mg_env_int("MG_BATCH_PLANES", 128);
     for (int i = 0; i < njobs; ++i) {
         mg::Job* j = nullptr;
         int rc = b->eng.add_job(jobs[i], -1, &j);

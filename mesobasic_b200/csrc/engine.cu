@@ -383,13 +383,22 @@ mg_tiling default_tiling(const Geometry& g, const DevInfo& d, int device)
 // Every job gets tiles of about kBatchThreads threads (ty + 2 mu rows of
 // nx/W strips), so the CTAs of one launch are equally full whatever each
 // job's row width; tiles are balanced to divide ny evenly; z chunks are about
-// 64 planes (16 rows for 2-D jobs; many jobs fill the grid, so no job is cut
-// finer).  A pure
+// kBatchPlanes planes (16 rows for 2-D jobs; many jobs fill the grid, so no
+// job is cut finer).  320 threads is the largest CTA that keeps two per SM
+// at 96 registers.  A pure
 // function of the shape: a job keeps its tiling for its whole life.
-mg_tiling batch_tiling_for(const Geometry& g, const DevInfo& d, int device)
+// environment knob: a positive integer, else `def`
+int mg_env_int(const char* name, int def)
+{
+    const char* e = std::getenv(name);
+    const int v = e ? std::atoi(e) : 0;
+    return v > 0 ? v : def;
+}
+
+mg_tiling batch_tiling_for(const Geometry& g, const DevInfo& d, int device, int threads, int planes)
 {
     if (!tma_shape_ok(g)) return default_tiling(g, d, device);
-    constexpr int kBatchThreads = 256;
+    const int kBatchThreads = std::max(32, threads), kBatchPlanes = std::max(1, planes);
     const int nq = g.lnx / (kStripBytes / g.es);
     const int nbuf = g.flat ? 8 : 4;
     int ty = 1;
@@ -403,7 +412,7 @@ mg_tiling batch_tiling_for(const Geometry& g, const DevInfo& d, int device)
     }
     // 2-D jobs march along their rows one row per plane: shorter chunks give
     // them enough CTAs
-    mg_tiling t{ty, std::max(1, g.lnz / (g.flat ? 16 : 64)), nbuf, 0};
+    mg_tiling t{ty, std::max(1, g.lnz / (g.flat ? 16 : kBatchPlanes)), nbuf, 0};
     TilePlan pl;
     while (plan_tiling(g, t, d, &pl) != MG_OK) {  // shrink the tile until it fits
         clear_error();
@@ -623,7 +632,7 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const mg
         return fail(MG_EINVAL, "the variable-mobility model runs in FP64 without mass feedback");
     MG_CUDA(cudaSetDevice(device));
     if (fh) j->tiling = mg_tiling{1, 1, 4, 1};  // the per-site path
-    else j->tiling = batch_tiling ? batch_tiling_for(j->g, info, device) : default_tiling(j->g, info, device);
+    else j->tiling = batch_tiling ? batch_tiling_for(j->g, info, device, batch_threads, batch_planes) : default_tiling(j->g, info, device);
     MG_TRY(plan_tiling(j->g, j->tiling, info, &j->plan));
     if (j->p.mass_correct && !j->plan.tma_ok)
         return fail(MG_EINVAL, "mass_correct needs a shape the tiled kernel takes (nx multiple of %d)", 32);

@@ -18,6 +18,7 @@ namespace mg {
 
 // ---- error reporting (thread-local message, C-ABI return codes)
 int fail(int code, const char* fmt, ...);
+int mg_env_int(const char* name, int def);  // a positive integer from the environment, else def
 void clear_error();
 const char* last_error();
 
@@ -117,6 +118,12 @@ class Engine {
     // jobs share launches (batch, server): tile every job for equally full
     // CTAs (batch_tiling_for) instead of for the fastest standalone run
     bool batch_tiling = false;
+    // threads per CTA and z-chunk length of that tiling: big tiles and long
+    // chunks (fewer, longer items) suit a batch that fills the GPU by
+    // itself; a server with few jobs in flight needs more, smaller items to
+    // spread each job over the SMs
+    int batch_threads = 320;
+    int batch_planes = 128;
     cudaStream_t stream = nullptr;
     DevInfo info;
     std::vector<Job*> jobs;
