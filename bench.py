@@ -152,6 +152,75 @@ def batch_jobs(mb, njobs=64, seed=7):
     return jobs
 
 
+# variable-mobility models at 256^3: parameters that keep the mobility off its
+# clamps, each model's own initial field (co + 0.1*(r - 0.5)) and its
+# reference default noise strength 0.1
+MODEL_LEG = (
+    ("TIPSphil", dict(alpha=150.0, beta=0.1, N=50.0, Tinit=300.0, Tbath=280.0, Tcrystal=200.0, gamma=1.0, D0=1.0,
+                      Mweight=0.5, Mvolume=1.0), 0.3),
+    ("TIPSbathPHIL", dict(alpha=150.0, beta=0.1, N=50.0, Tinit=320.0, Tbath=260.0, Tcrystal=200.0, gamma=1.0,
+                          D0=1.0, Mweight=0.5, Mvolume=1.0), 0.3),
+    ("SIPS", dict(Mweight=1.0, Mvolume=1.0, gamma=1.0), 0.1),
+    ("SIPSternary", dict(Kpp=1.0, Knn=1.0, Mpp=1.0, Mnn=1.0), 0.2),
+)
+
+
+def run_models(mb, torch, dev, steps, warmup, flush, sampler, peak):
+    """The variable-mobility steps (FP64, two passes: mu and mobility, then
+    div(mob grad mu) and the update; then the noise term) at 256^3, CUDA
+    events around each step, L2 flushed between steps.  GLUPS counts field
+    site updates (SIPSternary: two fields).  `achieved` is the algorithmic
+    16 B per site update (read c, write c'); the two-pass design moves 56 B
+    (pass 1: read c, write mu and mob; pass 2: read c, mu, mob, write c')
+    plus 16 B for the noise."""
+    n = N
+    sites = float(n) ** 3
+    out = {}
+    for name, kw, co in MODEL_LEG:
+        base = mb.ic_generate((n, n, n), 0.0, 0.1, False, SEED)
+        bc = (1, 1, 1) if name == "TIPSphil" else (0, 1, 1)
+        p = mb.make_params(n, n, n, 0.01, bc=bc, noise=0.1, noise_seed=SEED)
+        if name == "SIPSternary":
+            sim = mb.Ternary(p, dev, **kw)
+            sim.set_fields(co + base, 0.1 - base)
+            fields = 2
+        else:
+            if name == "SIPS":
+                sim = mb.CHSim(p, dev, sips=mb.make_sips_params(**kw))
+            else:
+                sim = mb.CHSim(p, dev, fh=mb.make_fh_params(10 ** 6, bath=name == "TIPSbathPHIL", **kw))
+            sim.set_field(co + base)
+            fields = 1
+        del base
+        ext = torch.cuda.ExternalStream(sim.stream, device=f"cuda:{dev}")
+        for _ in range(warmup):
+            sim.step(1)
+        sim.sync()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        torch.cuda.synchronize()
+        sampler.start()
+        for e0, e1 in evs:
+            with torch.cuda.stream(ext):
+                flush.fill_(1)
+            e0.record(ext)
+            sim.step(1)
+            e1.record(ext)
+        sim.sync()
+        torch.cuda.synchronize()
+        sampler.stop()
+        ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in evs)
+        sim.close()
+        upd = fields * sites
+        out[name] = {"value": upd / (ms * 1e-3) / 1e9, "unit": "GLUPS", "ms_per_step": ms,
+                     "achieved_gbs": upd * 16 / (ms * 1e-3) / 1e9, "frac": upd * 16 / (ms * 1e-3) / 1e9 / peak,
+                     "design_gbs": upd * 72 / (ms * 1e-3) / 1e9, "fields": fields}
+    out["workload"] = (f"{n}^3 FP64 per field, dt 0.01, noise 0.1, {steps} timed steps after {warmup} warm-up, "
+                       "L2 flushed between steps; TIPSphil periodic, the others no-flux x")
+    out["bytes"] = ("achieved: 16 B per site update (algorithmic); design_gbs: 72 B per site update "
+                    "(two passes 56 B + noise 16 B)")
+    return out
+
+
 def run_batch(mb, torch, dev, steps, sampler):
     import numpy as np
     jobs = batch_jobs(mb)
@@ -323,6 +392,8 @@ def run_ours(args, rank, world, local_rank):
         results[prec] = dict(ms_total=tot_ms, ms=ms, tiling=tiling)
     e2e_t = {prec: e2e(mb.make_params(N, N, N, DT, kappa=KAP, M=M, precision=prec), args.steps)
              for prec in ("fp64", "fp32")}
+    models = (run_models(mb, torch, dev, min(args.steps, 20), max(args.warmup, 3), flush, sampler, load_peaks()[0])
+              if args.model_steps else None)
     batch = run_batch(mb, torch, dev, args.batch_steps, sampler) if args.batch_steps > 0 else None
     clocks = sampler.summary()
     serve = run_serve(mb, dev, args.serve_seconds) if args.serve_seconds > 0 else None
@@ -375,6 +446,7 @@ def run_ours(args, rank, world, local_rank):
         "tiling": out["fp64"]["tiling"],
         "batch": batch,
         "serve": serve,
+        "models": models,
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": args.steps,
@@ -457,6 +529,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--batch-steps", type=int, default=1000, help="steps of the batched sweep (0: skip)")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the served stream (0: skip)")
+    ap.add_argument("--model-steps", type=int, default=1, help="time the variable-mobility models (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -177,14 +177,64 @@ typedef struct {
  * mass_correct 0); kappa is [PFApp/kap]; params->M is unused (the mobility
  * comes from the model); params->noise adds the reference's fluctuation term
  * (TIPSphil.cpp:200-209, [PFApp/noiseStr]).  Every other mg_ch_* call
- * applies.  Replaces: PFBaseClass::PFFactory returning TIPSphil
- * (PFBaseClass.cpp:43). */
+ * applies.  Replaces: PFBaseClass::PFFactory returning TIPSphil or
+ * TIPSbathPHIL (PFBaseClass.cpp:46-47). */
 int mg_fh_create(const mg_ch_params* params, const mg_fh_params* fh, int device, mg_ch_t** out);
 
 /* The mobility field of the last step taken (nx*ny*nz doubles, x fastest;
  * waits for enqueued work).  Replaces: the mob field TIPSphil writes at
  * PFApp/mobStep (TIPSphil.cpp:180-185). */
 int mg_fh_mobility(mg_ch_t* h, double* host);
+
+/* SIPS (SIPS.cpp): a binary polymer/solvent film in front of a non-solvent
+ * bath.  Keys of the reference input file in brackets, the reference defaults
+ * in parentheses (SIPS.cpp:22-59). */
+typedef struct {
+    double N;               /* polymer length [PFApp/N (100)] */
+    double A;               /* c <= 0 branch of mu [PFApp/A (1)] */
+    double Tinit;           /* kT = Tinit/273 [PFApp/Tinit (273.15)] */
+    double chiPS, chiPN;    /* polymer-solvent and polymer-non-solvent chi [PFApp/chiPS (0.034), chiPN (2.5)] */
+    double chiCond;         /* front diffusivity: chi = (chiPS-chiPN)*erf(i/(2*sqrt(chiCond*step*dt)))
+                               + chiPN for x >= NSdepth, chiPN below (SIPS.cpp:164-170)
+                               [PFApp/chiCond (1)] */
+    double phiCutoff;       /* no noise where c >= phiCutoff [PFApp/phiCutoff (0.5)] */
+    double nu, gamma;       /* Phillies law D0*exp(-gamma*phi^nu) [PFApp/nu (1), gamma (10)] */
+    double D0;              /* [PFApp/D0 (1)] */
+    double Mweight, Mvolume;/* phi -> g/L [PFApp/Mweight (100), Mvolume (0.1)] */
+    int NSdepth;            /* x planes of the non-solvent bath [PFApp/NSdepth (0)] */
+} mg_sips_params;
+
+/* A simulation stepped by SIPS::updatePhaseField (SIPS.cpp:130-249): the
+ * Flory-Huggins mu of the clamped concentration with chi(x, step) from the
+ * erf front, Phillies mobility over the second derivative, clamped to
+ * [1e-5, 1] and scaled by 0.95 + 0.25*log(1.0225 - (chi-chiPS)/(chiPN-chiPS)),
+ * then div(mob grad mu) as mg_fh_create's.  FP64 only; kappa is [PFApp/kap];
+ * params->M is unused; params->noise is [PFApp/noiseStr], skipped at sites
+ * with c >= phiCutoff after the step.  chiPS == chiPN is refused (the
+ * reference divides by their difference).  mg_fh_mobility returns the
+ * mobility.  Replaces: PFBaseClass::PFFactory returning SIPS
+ * (PFBaseClass.cpp:48). */
+int mg_sips_create(const mg_ch_params* params, const mg_sips_params* sips, int device, mg_ch_t** out);
+
+/* SIPSternary (SIPSternary.cpp): polymer c and non-solvent n [defaults
+ * SIPSternary.cpp:21-63]. */
+typedef struct {
+    double Kpp, Knn;        /* gradient coefficients [PFApp/Kpp (1), Knn (1)] */
+    double Mpp, Mnn;        /* mobilities [PFApp/Mpp (1), Mnn (1)] */
+} mg_ternary_params;
+
+/* The two fields of SIPSternary::updatePhaseField (SIPSternary.cpp:132-278)
+ * as a batch of two jobs: job 0 is the polymer c, job 1 the non-solvent n.
+ * In the reference the Flory-Huggins derivatives are assigned to variables
+ * declared inside their branches (SIPSternary.cpp:175-216), so the chemical
+ * potentials it uses are mu_c = 0.0 - Kpp*lap(c) and mu_n = 0.0 - Knn*lap(n),
+ * with constant mobilities Mpp and Mnn; each field takes c += dt*div(M grad
+ * mu) on its own, and that arithmetic is what runs here.  params->noise is
+ * [PFApp/noiseStr]: c gets dt*noise*(r - 0.5), n the same increment negated
+ * (SIPSternary.cpp:256-277).  FP64 only; params->kappa and M are unused.  The
+ * mg_batch_* calls apply.  Replaces: PFBaseClass::PFFactory returning
+ * SIPSternary (PFBaseClass.cpp:49). */
+int mg_ternary_create(const mg_ch_params* params, const mg_ternary_params* t, int device, mg_batch_t** out);
 
 /* Times candidate decompositions of `params` on `device` (scratch fields,
  * `trials` timed launches each) and returns the fastest.  Results are
@@ -223,6 +273,8 @@ int mg_batch_step(mg_batch_t* b, int nsteps);
 int mg_batch_sync(mg_batch_t* b, long long timeout_us);
 int mg_batch_get_field(mg_batch_t* b, int job, double* host);
 int mg_batch_reduce(mg_batch_t* b, int job, mg_ch_stats* out);
+/* mg_ch_write_vtk for one job of the batch. */
+int mg_batch_write_vtk(mg_batch_t* b, int job, const char* path, const char* tag, int iskip, int jskip, int kskip);
 void* mg_batch_stream(mg_batch_t* b);
 /* Items (tiles) and persistent CTAs of the batch's launches. */
 int mg_batch_info(const mg_batch_t* b, int* nitems, int* nctas, int* nlaunch_per_step);

@@ -17,10 +17,10 @@ import numpy as np
 
 from . import _lib
 from ._lib import (MG_FP32, MG_FP64, MG_JOB_DONE, MG_JOB_FAILED, MG_JOB_QUEUED, MG_JOB_RUNNING, MGError,
-                   FhParams, Params, ServerStats, Stats, Tiling, check, load)
+                   FhParams, Params, ServerStats, SipsParams, Stats, TernaryParams, Tiling, check, load)
 
-__all__ = ["CHSim", "Batch", "Server", "Params", "Stats", "Tiling", "MGError", "MG_FP32", "MG_FP64",
-           "make_params", "ic_generate", "vtk_write", "autotune", "load"]
+__all__ = ["CHSim", "Batch", "Ternary", "Server", "Params", "Stats", "Tiling", "MGError", "MG_FP32", "MG_FP64",
+           "make_params", "make_fh_params", "make_sips_params", "ic_generate", "vtk_write", "autotune", "load"]
 
 
 def make_params(nx, ny, nz, dt, kappa=1.0, M=1.0, dx=1.0, dy=1.0, dz=1.0, bc=(1, 1, 1),
@@ -63,18 +63,41 @@ def make_fh_params(nstep, bath=False, thermCond=1.0, **kw) -> FhParams:
     return FhParams(*(float(v[k]) for k in FH_DEFAULTS), int(nstep), int(bool(bath)), float(thermCond))
 
 
-class CHSim:
-    """One simulation on one GPU: the Cahn-Hilliard step, or with `fh`
-    (make_fh_params) the variable-mobility TIPSphil step."""
+# SIPS.cpp:22-59 (NSdepth is separate: an integer)
+SIPS_DEFAULTS = dict(N=100.0, A=1.0, Tinit=273.15, chiPS=0.034, chiPN=2.5, chiCond=1.0, phiCutoff=0.5, nu=1.0,
+                     gamma=10.0, D0=1.0, Mweight=100.0, Mvolume=0.1)
 
-    def __init__(self, params: Params, device: int = 0, fh: FhParams = None):
+
+def make_sips_params(NSdepth=0, **kw) -> SipsParams:
+    """SIPS parameters; unnamed ones take the reference's defaults."""
+    unknown = set(kw) - set(SIPS_DEFAULTS)
+    if unknown:
+        raise ValueError(f"unknown SIPS parameters {sorted(unknown)}")
+    v = dict(SIPS_DEFAULTS, **kw)
+    return SipsParams(*(float(v[k]) for k in SIPS_DEFAULTS), int(NSdepth))
+
+
+# SIPSternary.cpp:21-63
+TERNARY_DEFAULTS = dict(Kpp=1.0, Knn=1.0, Mpp=1.0, Mnn=1.0)
+
+
+class CHSim:
+    """One simulation on one GPU: the Cahn-Hilliard step; with `fh`
+    (make_fh_params) the variable-mobility TIPSphil step; with `sips`
+    (make_sips_params) the SIPS step."""
+
+    def __init__(self, params: Params, device: int = 0, fh: FhParams = None, sips: SipsParams = None):
         self._L = load()
         self.params = params
         h = ctypes.c_void_p()
-        if fh is None:
-            check(self._L.mg_ch_create(ctypes.byref(params), device, ctypes.byref(h)))
-        else:
+        if fh is not None and sips is not None:
+            raise ValueError("give fh or sips, not both")
+        if fh is not None:
             check(self._L.mg_fh_create(ctypes.byref(params), ctypes.byref(fh), device, ctypes.byref(h)))
+        elif sips is not None:
+            check(self._L.mg_sips_create(ctypes.byref(params), ctypes.byref(sips), device, ctypes.byref(h)))
+        else:
+            check(self._L.mg_ch_create(ctypes.byref(params), device, ctypes.byref(h)))
         self._h = h
 
     def mobility(self) -> np.ndarray:
@@ -173,6 +196,16 @@ class Batch:
         check(self._L.mg_batch_create(arr, len(self.params), device, ctypes.byref(h)))
         self._h = h
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def write_vtk(self, job: int, path, tag="c", iskip=1, jskip=1, kskip=1):
+        """Appends job's field to `path` as legacy VTK formatted on the GPU."""
+        check(self._L.mg_batch_write_vtk(self._h, job, str(path).encode(), tag.encode(), iskip, jskip, kskip))
+
     def close(self):
         if getattr(self, "_h", None):
             self._L.mg_batch_destroy(self._h)
@@ -211,6 +244,31 @@ class Batch:
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check(self._L.mg_batch_info(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return {"items": a.value, "ctas": b.value, "launches_per_step": c.value}
+
+
+class Ternary(Batch):
+    """SIPSternary's two fields, polymer c (job 0) and non-solvent n (job 1),
+    stepped as the reference's update computes them (mg_ternary_create);
+    `kw` takes Kpp, Knn, Mpp, Mnn (TERNARY_DEFAULTS)."""
+
+    def __init__(self, params: Params, device: int = 0, **kw):
+        unknown = set(kw) - set(TERNARY_DEFAULTS)
+        if unknown:
+            raise ValueError(f"unknown SIPSternary parameters {sorted(unknown)}")
+        v = dict(TERNARY_DEFAULTS, **kw)
+        self._L = load()
+        self.params = [params, params]
+        tp = TernaryParams(*(float(v[k]) for k in TERNARY_DEFAULTS))
+        h = ctypes.c_void_p()
+        check(self._L.mg_ternary_create(ctypes.byref(params), ctypes.byref(tp), device, ctypes.byref(h)))
+        self._h = h
+
+    def set_fields(self, c, n):
+        self.set_field(0, c)
+        self.set_field(1, n)
+
+    def get_fields(self):
+        return self.get_field(0), self.get_field(1)
 
 
 class Server:

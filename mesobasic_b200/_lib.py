@@ -48,6 +48,19 @@ class FhParams(ctypes.Structure):
                 ("bath", ctypes.c_int), ("thermCond", ctypes.c_double)]
 
 
+class SipsParams(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_double), ("A", ctypes.c_double), ("Tinit", ctypes.c_double),
+                ("chiPS", ctypes.c_double), ("chiPN", ctypes.c_double), ("chiCond", ctypes.c_double),
+                ("phiCutoff", ctypes.c_double), ("nu", ctypes.c_double), ("gamma", ctypes.c_double),
+                ("D0", ctypes.c_double), ("Mweight", ctypes.c_double), ("Mvolume", ctypes.c_double),
+                ("NSdepth", ctypes.c_int)]
+
+
+class TernaryParams(ctypes.Structure):
+    _fields_ = [("Kpp", ctypes.c_double), ("Knn", ctypes.c_double), ("Mpp", ctypes.c_double),
+                ("Mnn", ctypes.c_double)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("mass", ctypes.c_double), ("energy", ctypes.c_double), ("abs_mass", ctypes.c_double),
                 ("max_abs", ctypes.c_double), ("nonfinite", ctypes.c_longlong), ("step", ctypes.c_longlong)]
@@ -100,6 +113,8 @@ SIGNATURES = {
     "mg_ch_destroy": (None, [_vp]),
     "mg_fh_create": (ctypes.c_int, [_P(Params), _P(FhParams), ctypes.c_int, _P(_vp)]),
     "mg_fh_mobility": (ctypes.c_int, [_vp, _dp]),
+    "mg_sips_create": (ctypes.c_int, [_P(Params), _P(SipsParams), ctypes.c_int, _P(_vp)]),
+    "mg_ternary_create": (ctypes.c_int, [_P(Params), _P(TernaryParams), ctypes.c_int, _P(_vp)]),
     "mg_autotune": (ctypes.c_int, [_P(Params), ctypes.c_int, ctypes.c_int, _P(Tiling), _dp]),
     "mg_ic_generate": (ctypes.c_int, [_i3, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_uint, _dp]),
     "mg_vtk_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, _dp, _i3, ctypes.c_int, ctypes.c_int,
@@ -110,6 +125,8 @@ SIGNATURES = {
     "mg_batch_sync": (ctypes.c_int, [_vp, ctypes.c_longlong]),
     "mg_batch_get_field": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     "mg_batch_reduce": (ctypes.c_int, [_vp, ctypes.c_int, _P(Stats)]),
+    "mg_batch_write_vtk": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int]),
     "mg_batch_stream": (_vp, [_vp]),
     "mg_batch_info": (ctypes.c_int, [_vp, _P(ctypes.c_int), _P(ctypes.c_int), _P(ctypes.c_int)]),
     "mg_batch_destroy": (None, [_vp]),

@@ -25,6 +25,21 @@ struct mg_batch {
 
 using mg::fail;
 
+// a single variable-mobility simulation with model parameters f
+static int create_fh(const mg_ch_params* params, const mg::FhDev& f, int device, mg_ch_t** out)
+{
+    mg::Geometry g;
+    MG_TRY(mg::make_geometry(*params, &g));
+    if (params->precision != MG_FP64 || params->mass_correct)
+        return fail(MG_EINVAL, "the variable-mobility models run in FP64 without mass feedback");
+    std::unique_ptr<mg_ch> h(new (std::nothrow) mg_ch);
+    if (!h) return fail(MG_ENOMEM, "host allocation failed");
+    MG_TRY(h->eng.init(device, 1));
+    MG_TRY(h->eng.add_job(*params, -1, &h->job, &f));
+    *out = h.release();
+    return MG_OK;
+}
+
 extern "C" {
 
 const char* mg_last_error(void) { return mg::last_error(); }
@@ -57,13 +72,82 @@ int mg_fh_create(const mg_ch_params* params, const mg_fh_params* fh, int device,
     if (fh->bath != 0 && fh->bath != 1) return fail(MG_EINVAL, "bath must be 0 or 1");
     if (!std::isfinite(fh->thermCond)) return fail(MG_EINVAL, "thermCond must be finite");
     if (fh->N == 0 || fh->Mvolume == 0 || fh->Tinit == 0) return fail(MG_EINVAL, "N, Mvolume and Tinit must be nonzero");
+    mg::FhDev f{};
+    f.alpha = fh->alpha;
+    f.beta = fh->beta;
+    f.N = fh->N;
+    f.A = fh->A;
+    f.Tinit = fh->Tinit;
+    f.Tbath = fh->Tbath;
+    f.Tcrystal = fh->Tcrystal;
+    f.nu = fh->nu;
+    f.gamma = fh->gamma;
+    f.D0 = fh->D0;
+    f.Mweight = fh->Mweight;
+    f.Mvolume = fh->Mvolume;
+    f.nstep = fh->nstep;
+    f.model = fh->bath ? mg::kFhBath : mg::kFhRamp;
+    f.thermCond = fh->thermCond;
+    return create_fh(params, f, device, out);
+}
+
+int mg_sips_create(const mg_ch_params* params, const mg_sips_params* sp, int device, mg_ch_t** out)
+{
+    mg::clear_error();
+    if (!params || !sp || !out) return fail(MG_EINVAL, "null argument");
+    *out = nullptr;
+    const double v[12] = {sp->N,  sp->A,     sp->Tinit, sp->chiPS, sp->chiPN,   sp->chiCond,
+                          sp->phiCutoff, sp->nu, sp->gamma, sp->D0, sp->Mweight, sp->Mvolume};
+    for (double x : v)
+        if (!std::isfinite(x)) return fail(MG_EINVAL, "SIPS parameters must be finite");
+    if (sp->chiPS == sp->chiPN) return fail(MG_EINVAL, "chiPS and chiPN must differ (the mobility scale divides by chiPN - chiPS)");
+    if (sp->N == 0 || sp->Mvolume == 0) return fail(MG_EINVAL, "N and Mvolume must be nonzero");
+    mg::FhDev f{};
+    f.N = sp->N;
+    f.A = sp->A;
+    f.Tinit = sp->Tinit;
+    f.nu = sp->nu;
+    f.gamma = sp->gamma;
+    f.D0 = sp->D0;
+    f.Mweight = sp->Mweight;
+    f.Mvolume = sp->Mvolume;
+    f.nstep = 1;
+    f.model = mg::kFhSips;
+    f.chiPS = sp->chiPS;
+    f.chiPN = sp->chiPN;
+    f.chiCond = sp->chiCond;
+    f.NSdepth = sp->NSdepth;
+    f.phiCutoff = sp->phiCutoff;
+    return create_fh(params, f, device, out);
+}
+
+int mg_ternary_create(const mg_ch_params* params, const mg_ternary_params* t, int device, mg_batch_t** out)
+{
+    mg::clear_error();
+    if (!params || !t || !out) return fail(MG_EINVAL, "null argument");
+    *out = nullptr;
+    const double v[4] = {t->Kpp, t->Knn, t->Mpp, t->Mnn};
+    for (double x : v)
+        if (!std::isfinite(x)) return fail(MG_EINVAL, "SIPSternary parameters must be finite");
+    if (params->precision != MG_FP64 || params->mass_correct)
+        return fail(MG_EINVAL, "the SIPSternary step runs in FP64 without mass feedback");
     mg::Geometry g;
     MG_TRY(mg::make_geometry(*params, &g));
-    std::unique_ptr<mg_ch> h(new (std::nothrow) mg_ch);
-    if (!h) return fail(MG_ENOMEM, "host allocation failed");
-    MG_TRY(h->eng.init(device, 1));
-    MG_TRY(h->eng.add_job(*params, -1, &h->job, fh));
-    *out = h.release();
+    std::unique_ptr<mg_batch> b(new (std::nothrow) mg_batch);
+    if (!b) return fail(MG_ENOMEM, "host allocation failed");
+    MG_TRY(b->eng.init(device, 2));
+    for (int i = 0; i < 2; ++i) {
+        mg_ch_params p = *params;
+        p.kappa = i == 0 ? t->Kpp : t->Knn;
+        mg::FhDev f{};
+        f.nstep = 1;
+        f.model = mg::kFhLinear;
+        f.Mconst = i == 0 ? t->Mpp : t->Mnn;
+        mg::Job* j = nullptr;
+        MG_TRY(b->eng.add_job(p, -1, &j, &f, i == 1));
+        b->jobs.push_back(j);
+    }
+    *out = b.release();
     return MG_OK;
 }
 
@@ -321,6 +405,14 @@ int mg_batch_reduce(mg_batch_t* b, int job, mg_ch_stats* out)
     mg::Job* j;
     MG_TRY(batch_job(b, job, &j));
     return b->eng.diagnostics(j, out);
+}
+
+int mg_batch_write_vtk(mg_batch_t* b, int job, const char* path, const char* tag, int iskip, int jskip, int kskip)
+{
+    mg::clear_error();
+    mg::Job* j;
+    MG_TRY(batch_job(b, job, &j));
+    return b->eng.write_vtk(j, path, tag, iskip, jskip, kskip);
 }
 
 void* mg_batch_stream(mg_batch_t* b) { return b ? (void*)b->eng.stream : nullptr; }

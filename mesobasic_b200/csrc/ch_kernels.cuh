@@ -806,7 +806,10 @@ __global__ void ch_step_generic_kernel(JobDev* job)
 // ---------------------------------------------------------------------------
 // Per-step noise, the random fluctuation term of TIPSphil::updatePhaseField
 // (TIPSphil.cpp:200-209): after a step every site gets c += dt*(noise*(r -
-// 0.5)), each product rounded on its own as there.  The reference draws r
+// 0.5)), each product rounded on its own as there.  SIPS skips sites at or
+// above phiCutoff (SIPS.cpp:226-248); SIPSternary adds the negated increment
+// to its second field (SIPSternary.cpp:256-277), which a negative strength
+// with the same seed gives exactly.  The reference draws r
 // from rand(); here r comes from Philox4x32-10 (Salmon, Moraes, Dror, Shaw,
 // "Parallel random numbers: as easy as 1, 2, 3", SC 2011), keyed by the
 // job's seed, with counter (site / 4, step): four sites per draw, r =
@@ -844,7 +847,7 @@ __global__ void ch_noise_kernel(JobDev* job)
     if (!go) return;
     T* c = static_cast<T*>(J->buf[st & 1]);
     const long long n = (long long)J->nx * J->ny * J->nz;
-    const double noise = J->noise, dt = J->dtM_dt;
+    const double noise = J->noise, dt = J->dtM_dt, cutoff = J->noise_cutoff;
     const uint2 key = make_uint2((uint32_t)J->noise_seed, (uint32_t)(J->noise_seed >> 32));
     for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; 4 * g < n; g += (long long)gridDim.x * blockDim.x) {
         const uint4 w = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)(g >> 32), (uint32_t)st, (uint32_t)(st >> 32)), key);
@@ -854,10 +857,12 @@ __global__ void ch_noise_kernel(JobDev* job)
             const long long s = 4 * g + e;
             if (s >= n) break;
             const double r = __dadd_rn(__dmul_rn((double)word[e], 2.3283064365386963e-10), 1.1641532182693481e-10);
-            const double val = __dmul_rn(noise, __dsub_rn(r, 0.5));
+            const T cs = c[s];
+            // SIPS.cpp:239-240: no noise where c >= phiCutoff (the cutoff is +inf elsewhere)
+            const double val = (double)cs >= cutoff ? 0.0 : __dmul_rn(noise, __dsub_rn(r, 0.5));
             const double inc = __dmul_rn(dt, val);
-            if constexpr (sizeof(T) == 8) c[s] = __dadd_rn(c[s], inc);
-            else c[s] = c[s] + (float)inc;
+            if constexpr (sizeof(T) == 8) c[s] = __dadd_rn(cs, inc);
+            else c[s] = cs + (float)inc;
         }
     }
     __syncthreads();
@@ -871,17 +876,63 @@ __global__ void ch_noise_kernel(JobDev* job)
 }
 
 // ---------------------------------------------------------------------------
-// Variable-mobility step of TIPSphil::updatePhaseField (TIPSphil.cpp:113-211),
-// FP64, every operation rounded on its own in the reference's order; log,
-// exp, pow and sqrt are CUDA's (within an ulp or two of the host's libm).
-// Pass 1 stores mu and the mobility of every site; pass 2 forms the
-// harmonic-mean Laplacian of SfieldFD::Laplacian(const SfieldFD&)
-// (SfieldFD.cpp:333-355) and updates c.  Boundaries as the reference's
-// updateBoundaries: periodic axes wrap, a no-flux neighbour is the site itself.
+// Variable-mobility steps, FP64, every operation rounded on its own in the
+// reference's order; log, exp, pow, erf and sqrt are CUDA's (within an ulp or
+// two of the host's libm).  Pass 1 stores mu and the mobility of every site;
+// pass 2 forms the harmonic-mean Laplacian of SfieldFD::Laplacian(const
+// SfieldFD&) (SfieldFD.cpp:333-355) and updates c.  Boundaries as the
+// reference's updateBoundaries: periodic axes wrap, a no-flux neighbour is the
+// site itself.  The models (FhModel):
+//  - TIPSphil::updatePhaseField (TIPSphil.cpp:113-211) and TIPSbathPHIL's
+//    (TIPSbathPHIL.cpp:114-208): Flory-Huggins mu scaled by kT, Phillies
+//    mobility over the second derivative, crystallisation factor;
+//  - SIPS::updatePhaseField (SIPS.cpp:130-249): chi(x, step) from an erf
+//    front, mu from the clamped concentration, Phillies mobility scaled by
+//    0.95 + 0.25*log(1.0225 - chi fraction);
+//  - one field of SIPSternary::updatePhaseField (SIPSternary.cpp:132-278).
+//    There the Flory-Huggins derivatives are assigned to variables declared
+//    inside the branches (SIPSternary.cpp:175-216), which shadow the df_c and
+//    df_n that mu is formed from, so mu = 0.0 - K*lap(c) and the mobility is
+//    the constant Mpp (Mnn): the fields step independently.  The GPU takes
+//    the same arithmetic.
 
-__device__ __forceinline__ int fh_at(int x, int y, int z, const JobDev& J)
+__device__ __forceinline__ size_t fh_at(int x, int y, int z, const JobDev& J)
 {
-    return (z * J.ny + y) * J.nx + x;
+    return ((size_t)z * J.ny + y) * J.nx + x;
+}
+
+// SIPS: mu and mobility of one site (SIPS.cpp:160-208 with getFHcc,
+// philliesDiffusion and secondDerFH of SIPS.cpp:254-285)
+__device__ __forceinline__ void sips_site(const FhDev& F, double cc, double lapc, double kap, int x, double step,
+                                          double dt, double* mu, double* mob)
+{
+    using A = Arith<double>;
+    const double kT = A::div(F.Tinit, 273.0);
+    double chi;
+    if (x >= F.NSdepth)
+        chi = A::add(A::mul(A::sub(F.chiPS, F.chiPN),
+                            erf(A::div((double)(x + 1), A::mul(2.0, sqrt(A::mul(A::mul(F.chiCond, step), dt)))))),
+                     F.chiPN);
+    else
+        chi = F.chiPN;
+    const double cfh = cc < 0.0 ? 0.001 : (cc > 1.0 ? 0.999 : cc);
+    double df = A::add(A::sub(A::sub(A::div(A::add(log(cfh), 1.0), F.N), log(A::sub(1.0, cfh))), 1.0),
+                       A::mul(chi, A::sub(1.0, A::mul(2.0, cfh))));
+    if (cc <= 0.0) df = A::mul(A::mul(-1.5, F.A), sqrt(-cc));
+    *mu = A::sub(df, A::mul(kap, lapc));
+    double cphil;
+    if (cc >= 1.0) cphil = A::div(A::mul(1.0, F.Mweight), F.Mvolume);
+    else if (cc < 0.0) cphil = A::div(A::mul(0.000001, F.Mweight), F.Mvolume);
+    else cphil = A::div(A::mul(cc, F.Mweight), F.Mvolume);
+    double ddf = A::mul(0.5, A::add(A::div(1.0, A::mul(F.N, cc)), A::div(1.0, A::sub(1.0, cc))));
+    ddf = A::mul(ddf, kT);
+    const double Dp = A::mul(F.D0, exp(A::mul(-F.gamma, pow(cphil, F.nu))));
+    double Mc = A::div(Dp, ddf);
+    const double frac = A::div(A::sub(chi, F.chiPS), A::sub(F.chiPN, F.chiPS));
+    const double scale = A::add(0.95, A::mul(0.25, log(A::sub(1.0225, frac))));
+    if (Mc > 1.0) Mc = 1.0;
+    else if (Mc < 0.00001) Mc = 0.00001;
+    *mob = A::mul(Mc, scale);
 }
 
 __global__ void fh_mu_mob_kernel(JobDev* job)
@@ -894,19 +945,9 @@ __global__ void fh_mu_mob_kernel(JobDev* job)
     const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (J.step >= J.target || s >= n) return;
     const double* __restrict__ c = static_cast<const double*>(J.buf[J.step & 1]);
-    // temperature of the step being taken (PFApp passes it as current_step):
-    // a uniform ramp, or the bath profile along x (TIPSbathPHIL.cpp:118-121)
+    // the step being taken (PFApp passes it as current_step)
     const double cs = (double)(J.step + 1);
     const int x = (int)(s % nx), y = (int)((s / nx) % ny), z = (int)(s / ((size_t)nx * ny));
-    double T;
-    if (F.bath)
-        T = A::add(A::mul(A::sub(F.Tinit, F.Tbath),
-                          erf(A::div((double)(x + 1), A::mul(2.0, sqrt(A::mul(A::mul(F.thermCond, cs), J.dtM_dt)))))),
-                   F.Tbath);
-    else
-        T = A::sub(F.Tinit, A::mul(A::sub(F.Tinit, F.Tbath), A::div(cs, (double)F.nstep)));
-    const double kT = A::div(T, 273.0);
-    const double chi = A::add(A::div(F.alpha, T), F.beta);
     const bool pX = J.flags & JF_PER_X, pY = J.flags & JF_PER_Y, pZ = J.flags & JF_PER_Z;
     const double cc = c[s];
     const double xp = c[fh_at(wrap_or_clamp(x + 1, nx, pX), y, z, J)], xm = c[fh_at(wrap_or_clamp(x - 1, nx, pX), y, z, J)];
@@ -919,6 +960,26 @@ __global__ void fh_mu_mob_kernel(JobDev* job)
         lapc = A::add(A::add(axis_term(xp, xm, cc, J.cx, J.flags & JF_DIV_X), axis_term(yp, ym, cc, J.cy, J.flags & JF_DIV_Y)),
                       axis_term(zp, zm, cc, J.cz, J.flags & JF_DIV_Z));
     }
+    if (F.model == kFhLinear) {
+        F.mu[s] = A::sub(0.0, A::mul(J.kap, lapc));
+        F.mob[s] = F.Mconst;
+        return;
+    }
+    if (F.model == kFhSips) {
+        sips_site(F, cc, lapc, J.kap, x, cs, J.dtM_dt, F.mu + s, F.mob + s);
+        return;
+    }
+    // temperature of the step: a uniform ramp, or the bath profile along x
+    // (TIPSbathPHIL.cpp:118-121)
+    double T;
+    if (F.model == kFhBath)
+        T = A::add(A::mul(A::sub(F.Tinit, F.Tbath),
+                          erf(A::div((double)(x + 1), A::mul(2.0, sqrt(A::mul(A::mul(F.thermCond, cs), J.dtM_dt)))))),
+                   F.Tbath);
+    else
+        T = A::sub(F.Tinit, A::mul(A::sub(F.Tinit, F.Tbath), A::div(cs, (double)F.nstep)));
+    const double kT = A::div(T, 273.0);
+    const double chi = A::add(A::div(F.alpha, T), F.beta);
     // chemical potential: df = ((log(cc)+1)/N - log(1-cc) - 1 + chi*(1-2cc)) * kT
     double df = A::add(A::sub(A::sub(A::div(A::add(log(cc), 1.0), F.N), log(A::sub(1.0, cc))), 1.0),
                        A::mul(chi, A::sub(1.0, A::mul(2.0, cc))));
@@ -978,15 +1039,15 @@ __global__ void fh_update_kernel(JobDev* job)
     const int x = (int)(s % nx), y = (int)((s / nx) % ny), z = (int)(s / ((size_t)nx * ny));
     const bool pX = J.flags & JF_PER_X, pY = J.flags & JF_PER_Y, pZ = J.flags & JF_PER_Z;
     const double a0 = mu[s], bo = mob[s];
-    const int ixm = fh_at(wrap_or_clamp(x - 1, nx, pX), y, z, J), ixp = fh_at(wrap_or_clamp(x + 1, nx, pX), y, z, J);
-    const int izm = fh_at(x, y, wrap_or_clamp(z - 1, nz, pZ), J), izp = fh_at(x, y, wrap_or_clamp(z + 1, nz, pZ), J);
+    const size_t ixm = fh_at(wrap_or_clamp(x - 1, nx, pX), y, z, J), ixp = fh_at(wrap_or_clamp(x + 1, nx, pX), y, z, J);
+    const size_t izm = fh_at(x, y, wrap_or_clamp(z - 1, nz, pZ), J), izp = fh_at(x, y, wrap_or_clamp(z + 1, nz, pZ), J);
     const double lx = fh_axis(mu[ixm], mu[ixp], a0, mob[ixm], mob[ixp], bo, J.cx, J.flags & JF_DIV_X);
     const double lz = fh_axis(mu[izm], mu[izp], a0, mob[izm], mob[izp], bo, J.cz, J.flags & JF_DIV_Z);
     double lap;
     if (J.flags & JF_FLAT) {
         lap = A::add(lx, lz);
     } else {
-        const int iym = fh_at(x, wrap_or_clamp(y - 1, ny, pY), z, J), iyp = fh_at(x, wrap_or_clamp(y + 1, ny, pY), z, J);
+        const size_t iym = fh_at(x, wrap_or_clamp(y - 1, ny, pY), z, J), iyp = fh_at(x, wrap_or_clamp(y + 1, ny, pY), z, J);
         const double ly = fh_axis(mu[iym], mu[iyp], a0, mob[iym], mob[iyp], bo, J.cy, J.flags & JF_DIV_Y);
         lap = A::add(A::add(lx, ly), lz);
     }

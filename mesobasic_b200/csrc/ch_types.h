@@ -47,17 +47,33 @@ constexpr float kNudge = 1.1920928955078125e-7f;  // 2^-23
 // order).  A strip is the 8 sites x = 4t..4t+3 and nx/2 + 4t..4t+3 of a row.
 constexpr float kMassScale = 4294967296.0f;  // 2^32
 
-// Parameters and work fields of a variable-mobility (TIPSphil) job: the
-// Flory-Huggins chemical potential and Phillies mobility of
-// TIPSphil::updatePhaseField (TIPSphil.cpp:113-211), defaults of its
-// constructor (TIPSphil.cpp:41-59).
+// Which per-site chemical potential and mobility a variable-mobility job
+// takes (the update, div(mob grad mu) with harmonic-mean face mobilities, is
+// the same for all).
+enum FhModel : int {
+    kFhRamp = 0,    // TIPSphil::updatePhaseField (TIPSphil.cpp:113-211), uniform quench
+    kFhBath = 1,    // TIPSbathPHIL (TIPSbathPHIL.cpp:114-208), 1-D bath temperature along x
+    kFhSips = 2,    // SIPS::updatePhaseField (SIPS.cpp:130-249), erf non-solvent front along x
+    kFhLinear = 3,  // one field of SIPSternary::updatePhaseField (SIPSternary.cpp:132-278):
+                    // mu = 0.0 - K*lap(c), constant mobility
+};
+
+// Parameters and work fields of a variable-mobility job.  TIPSphil and
+// TIPSbathPHIL: the Flory-Huggins chemical potential and Phillies mobility
+// (constructor defaults TIPSphil.cpp:41-59); SIPS adds chiPS, chiPN, chiCond,
+// phiCutoff and NSdepth (SIPS.cpp:22-59); the SIPSternary field takes kappa as
+// its K and Mconst as its mobility.
 struct FhDev {
     double alpha, beta, N, A, Tinit, Tbath, Tcrystal, nu, gamma, D0, Mweight, Mvolume;
     long long nstep;  // Time/nstep: length of the temperature ramp
-    int bath;         // 1: temperature from the bath profile (TIPSbathPHIL)
+    int model;        // FhModel
     double thermCond;
     double* mu;       // chemical potential of the step being taken
     double* mob;      // mobility of the step being taken
+    double chiPS, chiPN, chiCond;  // SIPS: chi from chiPN (bath) toward chiPS behind an erf front
+    int NSdepth;                   // SIPS: planes x < NSdepth are the non-solvent bath (chi = chiPN)
+    double phiCutoff;              // SIPS: no noise where c >= phiCutoff after the step
+    double Mconst;                 // kFhLinear: the constant mobility
 };
 
 // Per-job state in device memory.  The host fills the parameters;
@@ -80,7 +96,8 @@ struct alignas(16) JobDev {
     long long nudge_count;      // sites in the window; the sign is the nudge's
     double mass_last;           // sum(c) after the last step (JF_MASS)
     FhDev* fh;                  // variable-mobility model (null: Cahn-Hilliard with constant M)
-    double noise;               // per-step noise strength (0: none)
+    double noise;               // per-step noise strength (0: none; negative: the increments negated)
+    double noise_cutoff;        // sites with c >= noise_cutoff after the step get no noise (SIPS)
     unsigned long long noise_seed;
     long long noise_step;       // the last step whose noise has been added
     unsigned int noise_done;    // blocks of the running noise launch finished

@@ -561,7 +561,8 @@ static void fill_jobdev(const Job& j, JobDev* jd)
     jd->kap = j.p.kappa;
     jd->dtM = j.p.dt * j.p.M;
     jd->dtM_dt = j.p.dt;
-    jd->noise = j.p.noise;
+    jd->noise = j.noise_negate ? -j.p.noise : j.p.noise;
+    jd->noise_cutoff = j.noise_cutoff;
     jd->noise_seed = j.p.noise_seed;
     jd->inv_nsites = 1.0 / (double)g.n;
     jd->target = j.target < 0 ? LLONG_MAX : j.target;
@@ -622,10 +623,12 @@ int Engine::init(int dev, int capacity)
     return MG_OK;
 }
 
-int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const mg_fh_params* fh)
+int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const FhDev* fh, bool noise_negate)
 {
     std::unique_ptr<Job> j(new Job);
     j->p = p;
+    j->noise_negate = noise_negate;
+    if (fh && fh->model == kFhSips) j->noise_cutoff = fh->phiCutoff;
     MG_TRY(make_geometry(p, &j->g));
     if (free_slots_.empty()) return fail(MG_ENOMEM, "no free job slot (capacity %d)", capacity_);
     if (fh && (p.precision != MG_FP64 || p.mass_correct))
@@ -647,8 +650,9 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const mg
         if (e == cudaSuccess) e = cudaMalloc(&j->d_mu, j->g.n * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&j->d_mob, j->g.n * sizeof(double));
         if (e == cudaSuccess) {
-            const FhDev f{fh->alpha, fh->beta, fh->N, fh->A, fh->Tinit, fh->Tbath, fh->Tcrystal, fh->nu, fh->gamma,
-                          fh->D0, fh->Mweight, fh->Mvolume, fh->nstep, fh->bath, fh->thermCond, j->d_mu, j->d_mob};
+            FhDev f = *fh;
+            f.mu = j->d_mu;
+            f.mob = j->d_mob;
             e = cudaMemcpy(j->d_fh, &f, sizeof f, cudaMemcpyHostToDevice);
         }
     }
@@ -676,6 +680,9 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const mg
             cudaFree(j->buf[1]);
             cudaFree(j->d_tmap);
             cudaFree(j->d_partial);
+            cudaFree(j->d_fh);
+            cudaFree(j->d_mu);
+            cudaFree(j->d_mob);
             return rc;
         }
     }

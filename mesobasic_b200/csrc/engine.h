@@ -79,9 +79,11 @@ struct Job {
     void* buf[2] = {nullptr, nullptr};
     CUtensorMap* d_tmap = nullptr;  // 4 maps
     long long* d_partial = nullptr;
-    FhDev* d_fh = nullptr;        // variable-mobility model (mg_fh_create)
+    FhDev* d_fh = nullptr;        // variable-mobility model (mg_fh_create, mg_sips_create, mg_ternary_create)
     double* d_mu = nullptr;       // its chemical potential ...
     double* d_mob = nullptr;      // ... and mobility fields
+    double noise_cutoff = __builtin_huge_val();  // no noise where c >= this after a step (SIPS)
+    bool noise_negate = false;    // add the negated noise increments (SIPSternary's second field)
     int slot = -1;
     long long target = -1;  // device step target (-1: unbounded)
     size_t device_bytes() const;
@@ -94,7 +96,10 @@ class Engine {
     int init(int device, int capacity);
 
     // job lifetime: allocate buffers + maps, take a slot
-    int add_job(const mg_ch_params& p, long long target, Job** out, const mg_fh_params* fh = nullptr);
+    // `fh`: a variable-mobility job; its parameters (mu and mob are set here).
+    // `noise_negate`: the job adds the negated noise increments.
+    int add_job(const mg_ch_params& p, long long target, Job** out, const FhDev* fh = nullptr,
+                bool noise_negate = false);
     int mobility(Job* j, double* host);  // last step's mobility (variable-mobility jobs)
     void remove_job(Job* j);  // releases the job; its device memory is freed at the next rebuild
     int set_tiling(Job* j, const mg_tiling& t);

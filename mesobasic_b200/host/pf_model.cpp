@@ -4,6 +4,7 @@
 #include <stdexcept>
 
 #include "chbasic_gpu.hpp"
+#include "sips_gpu.hpp"
 #include "tipsphil_gpu.hpp"
 
 PFBaseClass* PFBaseClass::PFFactory(const CommonParams& p, const InputFile& in)
@@ -13,9 +14,12 @@ PFBaseClass* PFBaseClass::PFFactory(const CommonParams& p, const InputFile& in)
     if (type == "CHBasic" || type == "CHBasicGPU") return new CHBasicGPU(p, in);
     if (type == "TIPSphil" || type == "TIPSphilGPU") return new TIPSphilGPU(p, in);
     if (type == "TIPSbathPHIL" || type == "TIPSbathPHILGPU") return new TIPSphilGPU(p, in, true);
+    if (type == "SIPS" || type == "SIPSGPU") return new SIPSGPU(p, in);
+    if (type == "SIPSternary" || type == "SIPSternaryGPU") return new SIPSternaryGPU(p, in);
     throw std::invalid_argument("PFApp/type '" + type +
                                 "' is not provided by this build (available: CHBasic, CHBasicGPU, TIPSphil, "
-                                "TIPSphilGPU, TIPSbathPHIL, TIPSbathPHILGPU)");
+                                "TIPSphilGPU, TIPSbathPHIL, TIPSbathPHILGPU, SIPS, SIPSGPU, SIPSternary, "
+                                "SIPSternaryGPU)");
 }
 
 PFApp::PFApp(const InputFile& in)

@@ -38,8 +38,9 @@ struct CommonParams {
 
 class PFBaseClass {
 public:
-    // "CHBasic"/"CHBasicGPU": the GPU Cahn-Hilliard model; "TIPSphil"/
-    // "TIPSphilGPU": the variable-mobility Flory-Huggins model
+    // "CHBasic"/"CHBasicGPU": the GPU Cahn-Hilliard model; "TIPSphil",
+    // "TIPSbathPHIL", "SIPS", "SIPSternary" (and their "...GPU" names): the
+    // variable-mobility models
     static PFBaseClass* PFFactory(const CommonParams&, const InputFile&);
 
     virtual void initPhaseField() = 0;

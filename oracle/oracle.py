@@ -87,6 +87,12 @@ def ref_lib():
         _ref.fhref_run.argtypes = [_i3, _d3, ctypes.c_double, _i3, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                    ctypes.c_int, _dp, ctypes.c_int, _dp]
         _ref.fhref_run.restype = ctypes.c_int
+        _ref.sipsref_run.argtypes = [_i3, _d3, ctypes.c_double, _i3, _dp, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int,
+                                     _dp]
+        _ref.sipsref_run.restype = ctypes.c_int
+        _ref.ternref_run.argtypes = [_i3, _d3, ctypes.c_double, _i3, _dp, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp,
+                                     _dp]
+        _ref.ternref_run.restype = ctypes.c_int
     return _ref
 
 
@@ -168,6 +174,38 @@ def fh_ref_run(c, dims, fh, nstep_total, first, nsteps, spacing=(1.0, 1.0, 1.0),
     ref_lib().fhref_run(_i3(*dims), _d3(*spacing), dt, _i3(*bc), _ptr(prm), int(bool(bath)), float(thermCond),
                         nstep_total, first, _ptr(a), nsteps, _ptr(out))
     return out
+
+
+# SIPS's parameters in the order sipsref_run takes them, with the reference
+# constructor's defaults (SIPS.cpp:22-59)
+SIPS_KEYS = ("N", "A", "Tinit", "chiPS", "chiPN", "chiCond", "phiCutoff", "nu", "gamma", "D0", "Mweight", "Mvolume",
+             "kap")
+SIPS_DEFAULTS = dict(N=100.0, A=1.0, Tinit=273.15, chiPS=0.034, chiPN=2.5, chiCond=1.0, phiCutoff=0.5, nu=1.0,
+                     gamma=10.0, D0=1.0, Mweight=100.0, Mvolume=0.1, kap=1.0)
+
+
+def sips_ref_run(c, dims, sp, first, nsteps, NSdepth=0, spacing=(1.0, 1.0, 1.0), dt=0.01, bc=(0, 1, 1)):
+    """Steps first..first+nsteps-1 of the reference's own SIPS update
+    (SIPS.cpp:130-249) on c, noise off; sp maps SIPS_KEYS to values."""
+    a = _as_field(c, dims)
+    out = np.empty_like(a)
+    prm = np.array([sp.get(k, SIPS_DEFAULTS[k]) for k in SIPS_KEYS], dtype=np.float64)
+    ref_lib().sipsref_run(_i3(*dims), _d3(*spacing), dt, _i3(*bc), _ptr(prm), int(NSdepth), first, _ptr(a), nsteps,
+                          _ptr(out))
+    return out
+
+
+def ternary_ref_run(c, n, dims, first, nsteps, Kpp=1.0, Knn=1.0, Mpp=1.0, Mnn=1.0, spacing=(1.0, 1.0, 1.0), dt=0.01,
+                    bc=(0, 1, 1)):
+    """Steps first..first+nsteps-1 of the reference's own SIPSternary update
+    (SIPSternary.cpp:132-278) on the fields c and n, noise off."""
+    a = _as_field(c, dims)
+    b = _as_field(n, dims)
+    oc, on = np.empty_like(a), np.empty_like(b)
+    prm = np.array([Kpp, Knn, Mpp, Mnn], dtype=np.float64)
+    ref_lib().ternref_run(_i3(*dims), _d3(*spacing), dt, _i3(*bc), _ptr(prm), first, _ptr(a), _ptr(b), nsteps,
+                          _ptr(oc), _ptr(on))
+    return oc, on
 
 
 def ref_ic(dims, co, amp, gaussian=False, seed=42) -> np.ndarray:

@@ -52,6 +52,30 @@ def test_create_rejects_bad_params_before_device_work(bad):
     assert not h.value
 
 
+@pytest.mark.parametrize("bad", [dict(chiPN=0.034), dict(N=float("nan")), dict(Mvolume=0.0), dict(prec="fp32"),
+                                 dict(nx=0)])
+def test_sips_create_rejects_bad_params_before_device_work(bad):
+    bad = dict(bad)
+    p = mb.make_params(bad.pop("nx", 8), 8, 8, 0.01, precision=bad.pop("prec", "fp64"))
+    sp = mb.make_sips_params(**bad)
+    h = ctypes.c_void_p()
+    assert mb.load().mg_sips_create(ctypes.byref(p), ctypes.byref(sp), 0, ctypes.byref(h)) == _lib.MG_EINVAL
+    assert not h.value
+
+
+@pytest.mark.parametrize("bad", [dict(Kpp=float("inf")), dict(Mnn=float("nan")), dict(prec="fp32"), dict(nx=-1)])
+def test_ternary_create_rejects_bad_params_before_device_work(bad):
+    bad = dict(bad)
+    p = mb.make_params(bad.pop("nx", 8), 8, 8, 0.01, precision=bad.pop("prec", "fp64"))
+    v = dict(mb.TERNARY_DEFAULTS, **bad)
+    tp = _lib.TernaryParams(*(v[k] for k in mb.TERNARY_DEFAULTS))
+    h = ctypes.c_void_p()
+    assert mb.load().mg_ternary_create(ctypes.byref(p), ctypes.byref(tp), 0, ctypes.byref(h)) == _lib.MG_EINVAL
+    assert not h.value
+    with pytest.raises(ValueError):
+        mb.make_sips_params(chi=1.0)
+
+
 def test_batch_rejects_bad_job():
     good = mb.make_params(8, 8, 8, 0.01)
     bad = mb.make_params(8, 0, 8, 0.01)

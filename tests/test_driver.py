@@ -72,8 +72,9 @@ def run_driver(tmp_path, text, *args, timeout=300):
 
 
 def test_unknown_model_type_fails_loudly(tmp_path):
-    r = run_driver(tmp_path, "[Domain]\nnx=8\n[]\n[PFApp]\napp = true\ntype = SIPS\n[]\n")
-    assert r.returncode == 1 and "SIPS" in r.stderr
+    # CHTernary: a type the reference's factory has commented out
+    r = run_driver(tmp_path, "[Domain]\nnx=8\n[]\n[PFApp]\napp = true\ntype = CHTernary\n[]\n")
+    assert r.returncode == 1 and "CHTernary" in r.stderr and "SIPSternary" in r.stderr
 
 
 def test_more_outputs_than_steps_is_an_error(tmp_path):
