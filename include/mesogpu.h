@@ -46,12 +46,16 @@ typedef struct {
     int bx, by, bz;        /* 1 periodic, 0 no-flux [PFApp/bx,by,bz] (SfieldFD.cpp:187-251) */
     int precision;         /* MG_FP64: bit-identical to the reference build;
                               MG_FP32: FP32 field, FP64 reductions */
-    int mass_correct;      /* MG_FP32 only: after each step the kernel sums the
-                              stored field in FP64, and the next step adds the
-                              defect (target - sum) back as exact nudges of
-                              2^-23 on a window of sites that moves every step,
-                              so rounding errors of the field do not accumulate
-                              as a drift of total mass */
+    int mass_correct;      /* MG_FP32 only; 0: off.  K >= 1: after every K-th
+                              step the kernel sums the stored field in FP64,
+                              and the next step adds the defect (target - sum)
+                              back as exact nudges of 2^-23 on a window of
+                              sites that moves at every measurement, so
+                              rounding errors of the field do not accumulate
+                              as a drift of total mass.  K = 1 measures every
+                              step; the Python mirror and the driver default
+                              to K = 4, which bounds the drift by four steps
+                              of rounding noise at a quarter of the cost */
     double noise;          /* >0: after each step every site gets
                               c += dt * (noise * (u - 0.5)), u uniform in (0,1)
                               [PFApp/noiseStr] (TIPSphil.cpp:200-209); 0: off */

@@ -23,11 +23,15 @@ __all__ = ["CHSim", "Batch", "Ternary", "Server", "Params", "Stats", "Tiling", "
            "make_params", "make_fh_params", "make_sips_params", "ic_generate", "vtk_write", "autotune", "load"]
 
 
+# FP32 mass feedback cadence: the stored field is summed after every 4th step
+MASS_EVERY = 4
+
+
 def make_params(nx, ny, nz, dt, kappa=1.0, M=1.0, dx=1.0, dy=1.0, dz=1.0, bc=(1, 1, 1),
                 precision="fp64", mass_correct=None, noise=0.0, noise_seed=0) -> Params:
     prec = MG_FP32 if precision in ("fp32", MG_FP32) else MG_FP64
     if mass_correct is None:
-        mass_correct = 1 if prec == MG_FP32 else 0
+        mass_correct = MASS_EVERY if prec == MG_FP32 else 0
     return Params(nx, ny, nz, dx, dy, dz, dt, M, kappa, bc[0], bc[1], bc[2], prec, int(mass_correct), float(noise),
                   int(noise_seed))
 

@@ -257,7 +257,7 @@ __device__ __forceinline__ int find_job(const int* item_begin, int njobs, int it
 
 // The stored mass of one thread strip in 2^-32 units: its 8 values summed
 // in FP64 (exact conversions, fixed order), rounded once.  The same function
-// measures the field at upload and after every step.
+// measures the field at upload and after every measured step.
 __device__ __forceinline__ long long strip_mass(float o0, float o1, float o2, float o3, float o4, float o5, float o6,
                                                 float o7)
 {
@@ -322,6 +322,9 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
         }
         __syncthreads();
         const long long step = head->step;
+        // this step's stored field is summed (mass feedback) on every
+        // mass_every-th step; the nudges it yields go into the next step
+        const bool measure = MASS && (step + 1) % J->mass_every == 0;
         if (step >= J->target) {  // uniform: read once by thread 0
             __syncthreads();        // head->step is rewritten for the next item
             continue;
@@ -599,7 +602,7 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
 #pragma unroll
                                 for (int k = 0; k < 4; ++k) out.p[k] = pk2(o[2 * k], o[2 * k + 1]);
                             }
-                            macc += strip_mass(out.get(0), out.get(1), out.get(2), out.get(3), out.get(4), out.get(5),
+                            if (measure) macc += strip_mass(out.get(0), out.get(1), out.get(2), out.get(3), out.get(4), out.get(5),
                                                out.get(6), out.get(7));
                         }
                     } else {
@@ -641,7 +644,7 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
 #pragma unroll
                                     for (int e = 0; e < 8; ++e) o[e] = t[e];
                                 }
-                                macc += strip_mass(o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7]);
+                                if (measure) macc += strip_mass(o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7]);
                             }
 #pragma unroll
                             for (int k = 0; k < 4; ++k) out.p[k] = pk2(o[2 * k], o[2 * k + 1]);
@@ -690,7 +693,7 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
 
         // ---- item epilogue: partial mass, completion count, last-item work
         const int nitems_job = J->ntile * J->nchunk;
-        if constexpr (MASS) {
+        if (measure) {
             // |strip| < 2^36 units, a thread holds at most nz strips, a CTA
             // at most 640 threads: the item sum fits 64 bits
             long long* red = reinterpret_cast<long long*>(head->red);
@@ -716,7 +719,8 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
         }
         __syncthreads();
         if (head->flag) {
-            if (MASS && tid < 32) {
+            if (MASS && !measure && tid == 0) J->nudge_count = 0;  // this step's nudges are spent
+            if (measure && tid < 32) {
                 __int128 r = 0;
                 for (int k = lane; k < nitems_job; k += 32) r += __ldcg(J->partial + k);
 #pragma unroll

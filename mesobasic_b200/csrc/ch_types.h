@@ -31,10 +31,10 @@ enum DeviceError : int {
     DEV_TMA_TIMEOUT = 1,  // a TMA completion wait ran out of polls
 };
 
-// FP32 mass feedback: after each step the kernel sums the stored field in
-// FP64; the defect D = target - sum becomes K = round(D / kNudge) nudges of
-// +-kNudge, which the next step adds to K consecutive sites (a window whose
-// start moves by a fixed stride every step).  kNudge = 2^-23 is a multiple
+// FP32 mass feedback: after every mass_every-th step the kernel sums the
+// stored field in FP64; the defect D = target - sum becomes K = round(D /
+// kNudge) nudges of +-kNudge, which the next step adds to K consecutive sites
+// (a window whose start moves by a fixed stride at every measurement).  kNudge = 2^-23 is a multiple
 // of the unit in the last place of every float below 2 in magnitude, so each
 // nudge is exact there and the stored sum meets the target to within one
 // step's rounding.
@@ -94,7 +94,8 @@ struct alignas(16) JobDev {
     double mass_target;         // sum(c) of the uploaded field (JF_MASS)
     long long nudge_begin;      // first site of the next step's nudge window (JF_MASS)
     long long nudge_count;      // sites in the window; the sign is the nudge's
-    double mass_last;           // sum(c) after the last step (JF_MASS)
+    double mass_last;           // sum(c) after the last measured step (JF_MASS)
+    int mass_every;             // JF_MASS: the field is summed after steps s with (s + 1) % mass_every == 0
     FhDev* fh;                  // variable-mobility model (null: Cahn-Hilliard with constant M)
     double noise;               // per-step noise strength (0: none; negative: the increments negated)
     double noise_cutoff;        // sites with c >= noise_cutoff after the step get no noise (SIPS)

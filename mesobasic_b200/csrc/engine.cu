@@ -2,6 +2,7 @@
 // graphs, transfers, diagnostics.  See engine.h.
 #include "engine.h"
 #include "ch_kernels.cuh"
+#include "ch_lean.cuh"
 
 #include <cufft.h>
 #include <dlfcn.h>
@@ -244,6 +245,25 @@ static StepKernel pick_maxt(int nbuf, int /*block*/)
 }
 
 // row widths with a compile-time specialisation of the step kernel
+// FP32 rows whose threads form a power-of-two segment of a warp take the
+// lean variant (bit-identical results, less per-plane overhead)
+template <bool MASS>
+static StepKernel pick_lean(int nx, int nbuf)
+{
+    switch (nx) {
+    case 64: return nbuf == 4 ? ch_lean_kernel<64, 4, MASS> : nullptr;
+    case 128: return nbuf == 4 ? ch_lean_kernel<128, 4, MASS> : nullptr;
+    case 256:
+        switch (nbuf) {
+        case 3: return ch_lean_kernel<256, 3, MASS>;
+        case 4: return ch_lean_kernel<256, 4, MASS>;
+        case 6: return ch_lean_kernel<256, 6, MASS>;
+        default: return ch_lean_kernel<256, 8, MASS>;
+        }
+    default: return nullptr;
+    }
+}
+
 template <typename T, bool FLAT, bool MASS>
 static StepKernel pick_fixed(int nx, int nbuf)
 {
@@ -270,6 +290,10 @@ static StepKernel pick_shape(bool flat, bool simple, int nbuf, int block)
 
 StepKernel step_kernel(bool fp32, bool flat, int nbuf, bool simple, int block, bool mass, int nx)
 {
+    if (fp32 && simple && !flat && nx > 0) {
+        StepKernel k = mass ? pick_lean<true>(nx, nbuf) : pick_lean<false>(nx, nbuf);
+        if (k) return k;
+    }
     if (simple && !flat && (nbuf == 4 || nbuf == 8) && nx > 0) {
         StepKernel k = fp32 ? (mass ? pick_fixed<float, false, true>(nx, nbuf) : pick_fixed<float, false, false>(nx, nbuf))
                             : pick_fixed<double, false, false>(nx, nbuf);
@@ -540,6 +564,7 @@ static void fill_jobdev(const Job& j, JobDev* jd)
     if (g.perz) flags |= JF_PER_Z;
     if (g.flat) flags |= JF_FLAT;
     if (j.p.mass_correct && g.es == 4) flags |= JF_MASS;
+    jd->mass_every = std::max(j.p.mass_correct, 1);
     if (geometry_simple(g)) flags |= JF_SIMPLE;
     const double sp[3] = {g.lsx, g.lsy, g.lsz};
     double coef[3];
