@@ -329,7 +329,7 @@ def run_ours(args, rank, world, local_rank):
 
     ic = mb.ic_generate((N, N, N), CO, AMP, False, SEED)
     flush_w = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
-    flush_r = torch.ones(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+    flush_r = torch.ones(64 << 20, dtype=torch.float32, device=f"cuda:{dev}")  # 256 MB
 
     class _Flush:
         """L2 flush between timed steps: a write larger than L2, then a read
