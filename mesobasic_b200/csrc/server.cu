@@ -209,8 +209,11 @@ int mg_server_create(int device, double hbm_budget_gb, int max_jobs_in_flight, i
     if (!s) return fail(MG_ENOMEM, "host allocation failed");
     MG_TRY(s->eng.init(device, max_jobs_in_flight));
     s->eng.batch_tiling = true;
-    s->eng.batch_threads = mg::mg_env_int("MG_SERVER_THREADS", 256);
-    s->eng.batch_planes = mg::mg_env_int("MG_SERVER_PLANES", 16);
+    // tile target of the served jobs: 320 threads a CTA and 64-plane z
+    // chunks took 11 % less GPU time on the served stream than 256 / 16
+    // (four settings measured back to back on one B200)
+    s->eng.batch_threads = mg::mg_env_int("MG_SERVER_THREADS", 320);
+    s->eng.batch_planes = mg::mg_env_int("MG_SERVER_PLANES", 64);
     s->budget = hbm_budget_gb * 1e9;
     s->max_inflight = max_jobs_in_flight;
     s->steps_per_tick = steps_per_tick > 0 ? steps_per_tick : 100;
