@@ -47,15 +47,17 @@ typedef struct {
     int precision;         /* MG_FP64: bit-identical to the reference build;
                               MG_FP32: FP32 field, FP64 reductions */
     int mass_correct;      /* MG_FP32 only; 0: off.  K >= 1: after every K-th
-                              step the kernel sums the stored field in FP64,
-                              and the next step adds the defect (target - sum)
-                              back as exact nudges of 2^-23 on a window of
-                              sites that moves at every measurement, so
-                              rounding errors of the field do not accumulate
-                              as a drift of total mass.  K = 1 measures every
-                              step; the Python mirror and the driver default
-                              to K = 4, which bounds the drift by four steps
-                              of rounding noise at a quarter of the cost */
+                              step the kernel sums the stored field in FP64
+                              and adds the defect (target - sum) back at once
+                              as exact nudges of 2^-23 on a window of sites;
+                              the steps in between add the rounding defect
+                              per step the last interval showed, so rounding
+                              errors of the field do not accumulate as a
+                              drift of total mass.  The stored mass is on
+                              target (to half a nudge) after every K-th step.
+                              K = 1 measures every step; the Python mirror
+                              and the driver default to K = 4, at a quarter
+                              of the measuring cost */
     double noise;          /* >0: after each step every site gets
                               c += dt * (noise * (u - 0.5)), u uniform in (0,1)
                               [PFApp/noiseStr] (TIPSphil.cpp:200-209); 0: off */

@@ -282,6 +282,73 @@ __device__ __noinline__ void nudge_strip(float* o, long long site0, long long of
     }
 }
 
+// FP32 mass feedback at the end of a step, run by the whole CTA that
+// finished the job's last item of the step (every item has stored its part
+// of the new field and fenced it).  The nudges this step added inside the
+// stencil are booked.  On a measured step the stored mass M (the items'
+// partial sums in item order) gives:
+//  - the correction: round((target - M) / kNudge) nudges, added here to
+//    consecutive sites of the new field, so the stored mass leaves every
+//    measured step on target;
+//  - the rounding defect of the interval since the last measure (the change
+//    of stored mass the nudges did not make), d per step: each step of the
+//    coming interval adds round(-d / kNudge) nudges inside the stencil, so
+//    the mass stays on target between measures while rounding losses are
+//    systematic (they are while the field evolves slowly).
+// kNudge is a multiple of the unit in the last place of every float below 2
+// in magnitude, so each nudge moves the stored sum by exactly its size.  The
+// window of nudged sites moves on by a golden-ratio fraction of the field
+// every step.
+__device__ __forceinline__ void mass_feedback_step_end(JobDev* J, bool measure, long long nsites, int nitems_job,
+                                                       float* field, SmemHead* head)
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    const long long stride = (long long)(0.6180339887498949 * (double)nsites) | 1;
+    if (tid < 32) {
+        __int128 r = 0;
+        if (measure) {
+            for (int k = lane; k < nitems_job; k += 32) r += __ldcg(J->partial + k);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const unsigned long long lo = __shfl_down_sync(0xffffffffu, (unsigned long long)r, off);
+                const long long hi = __shfl_down_sync(0xffffffffu, (long long)(r >> 64), off);
+                r += ((__int128)hi << 64) | (__int128)lo;
+            }
+        }
+        if (lane == 0) {
+            J->nudge_applied += J->nudge_count;
+            long long now = 0;
+            if (measure) {
+                const double mm = (double)r / (double)kMassScale;
+                const double d =
+                    ((mm - J->mass_last) - (double)J->nudge_applied * (double)kNudge) / (double)J->mass_every;
+                double k = rint((J->mass_target - mm) / (double)kNudge);
+                double kr = rint(-d / (double)kNudge);
+                k = fmin(fmax(k, -(double)nsites), (double)nsites);
+                kr = fmin(fmax(kr, -(double)nsites), (double)nsites);
+                now = (long long)k;
+                J->mass_last = mm + k * (double)kNudge;
+                J->nudge_applied = 0;
+                J->nudge_rest = (long long)kr;
+            }
+            head->nudge_begin = J->nudge_begin;
+            head->nudge_count = now;
+            const long long w = now != 0 ? (J->nudge_begin + stride) % nsites : J->nudge_begin;
+            J->nudge_count = J->nudge_rest;
+            J->nudge_begin = (w + stride) % nsites;
+        }
+    }
+    __syncthreads();
+    const long long cnt = head->nudge_count, w0 = head->nudge_begin;
+    const long long na = cnt < 0 ? -cnt : cnt;
+    const float nudge = cnt < 0 ? -kNudge : kNudge;
+    for (long long q = tid; q < na; q += blockDim.x) {
+        long long site = w0 + q;
+        if (site >= nsites) site -= nsites;
+        field[site] = __ldcg(field + site) + nudge;
+    }
+}
+
 // NXC: row width fixed at compile time (0: read from the job), so that row,
 // half and piece offsets fold into instruction immediates.
 template <typename T, int NBUF, bool FLAT, bool SIMPLE, bool MASS, int NXC = 0>
@@ -710,6 +777,7 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
                 if (lane == 0) J->partial[local] = r;
             }
         }
+        if (measure) __threadfence();  // this item's part of the new field, before the completion count
         __syncthreads();
         if (tid == 0) {
             __threadfence();
@@ -719,29 +787,9 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
         }
         __syncthreads();
         if (head->flag) {
-            if (MASS && !measure && tid == 0) J->nudge_count = 0;  // this step's nudges are spent
-            if (measure && tid < 32) {
-                __int128 r = 0;
-                for (int k = lane; k < nitems_job; k += 32) r += __ldcg(J->partial + k);
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1) {
-                    const unsigned long long lo = __shfl_down_sync(0xffffffffu, (unsigned long long)r, off);
-                    const long long hi = __shfl_down_sync(0xffffffffu, (long long)(r >> 64), off);
-                    r += ((__int128)hi << 64) | (__int128)lo;
-                }
-                if (lane == 0) {
-                    const double mm = (double)r / (double)kMassScale;
-                    J->mass_last = mm;
-                    // nudges for the next step; the window moves on by a
-                    // golden-ratio fraction of the field
-                    const long long nsites = (long long)pstride * nz;
-                    double k = rint((J->mass_target - mm) / (double)kNudge);
-                    k = fmin(fmax(k, -(double)nsites), (double)nsites);
-                    J->nudge_count = (long long)k;
-                    const long long stride = (long long)(0.6180339887498949 * (double)nsites) | 1;
-                    J->nudge_begin = (J->nudge_begin + stride) % nsites;
-                }
-            }
+            if constexpr (MASS)
+                mass_feedback_step_end(J, measure, (long long)pstride * nz, nitems_job, reinterpret_cast<float*>(dst),
+                                       head);
             if (tid == 0) {
                 J->done = 0;
                 J->step = step + 1;
@@ -1074,6 +1122,8 @@ __global__ void ch_job_reset(JobDev* job, long long target)
         job->err = 0;
         job->nudge_begin = 0;
         job->nudge_count = 0;
+        job->nudge_applied = 0;
+        job->nudge_rest = 0;
         job->noise_step = 0;
         job->noise_done = 0;
     }
@@ -1230,6 +1280,8 @@ __global__ void ch_mass_final(const long long* part, int nblocks, JobDev* job)
     job->mass_last = m;
     job->nudge_begin = 0;
     job->nudge_count = 0;
+    job->nudge_applied = 0;
+    job->nudge_rest = 0;
 }
 
 }  // namespace mg

@@ -328,6 +328,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1) ch_lean_kernel(StepArgs a)
                 if (lane == 0) J->partial[local] = r;
             }
         }
+        if (measure) __threadfence();  // this item's part of the new field, before the completion count
         __syncthreads();
         if (tid == 0) {
             __threadfence();
@@ -337,27 +338,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1) ch_lean_kernel(StepArgs a)
         }
         __syncthreads();
         if (head->flag) {
-            if (MASS && !measure && tid == 0) J->nudge_count = 0;  // this step's nudges are spent
-            if (measure && tid < 32) {
-                __int128 r = 0;
-                for (int k = lane; k < nitems_job; k += 32) r += __ldcg(J->partial + k);
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1) {
-                    const unsigned long long lo = __shfl_down_sync(0xffffffffu, (unsigned long long)r, off);
-                    const long long hi = __shfl_down_sync(0xffffffffu, (long long)(r >> 64), off);
-                    r += ((__int128)hi << 64) | (__int128)lo;
-                }
-                if (lane == 0) {
-                    const double mm = (double)r / (double)kMassScale;
-                    J->mass_last = mm;
-                    const long long nsites = (long long)pstride * nz;
-                    double k = rint((J->mass_target - mm) / (double)kNudge);
-                    k = fmin(fmax(k, -(double)nsites), (double)nsites);
-                    J->nudge_count = (long long)k;
-                    const long long stride = (long long)(0.6180339887498949 * (double)nsites) | 1;
-                    J->nudge_begin = (J->nudge_begin + stride) % nsites;
-                }
-            }
+            if constexpr (MASS) mass_feedback_step_end(J, measure, (long long)pstride * nz, nitems_job, dst, head);
             if (tid == 0) {
                 J->done = 0;
                 J->step = step + 1;

@@ -32,9 +32,14 @@ enum DeviceError : int {
 };
 
 // FP32 mass feedback: after every mass_every-th step the kernel sums the
-// stored field in FP64; the defect D = target - sum becomes K = round(D /
-// kNudge) nudges of +-kNudge, which the next step adds to K consecutive sites
-// (a window whose start moves by a fixed stride at every measurement).  kNudge = 2^-23 is a multiple
+// stored field in FP64 and adds round((target - sum) / kNudge) nudges of
+// kNudge to consecutive sites of the new field at once.  The rounding defect
+// of the interval since the last measure (the change of stored mass the
+// nudges did not make) gives a per-step defect d, and each step of the next
+// interval adds round(-d / kNudge) nudges inside the stencil (a window whose
+// start moves by a fixed stride every step).  Rounding losses are systematic
+// while the field evolves slowly, so predicting them keeps the stored mass
+// on target between measurements.  kNudge = 2^-23 is a multiple
 // of the unit in the last place of every float below 2 in magnitude, so each
 // nudge is exact there and the stored sum meets the target to within one
 // step's rounding.
@@ -95,6 +100,8 @@ struct alignas(16) JobDev {
     long long nudge_begin;      // first site of the next step's nudge window (JF_MASS)
     long long nudge_count;      // sites in the window; the sign is the nudge's
     double mass_last;           // sum(c) after the last measured step (JF_MASS)
+    long long nudge_applied;    // nudges (signed count) applied since the last measured step
+    long long nudge_rest;       // nudges for each unmeasured step of the interval (signed count)
     int mass_every;             // JF_MASS: the field is summed after steps s with (s + 1) % mass_every == 0
     FhDev* fh;                  // variable-mobility model (null: Cahn-Hilliard with constant M)
     double noise;               // per-step noise strength (0: none; negative: the increments negated)

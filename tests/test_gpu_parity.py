@@ -180,6 +180,24 @@ def test_fp32_mass_feedback_bounds_drift(every):
             assert abs(r["mass"] - m0) / abs(m0) <= 1e-10, r
 
 
+@pytest.mark.parametrize("every", [1, 4])
+def test_fp32_mass_feedback_bounds_drift_early_coarsening(every):
+    # a job of the batched sweep (128^3, c0 = 0.248, kappa = 0.705, uniform
+    # noise of amplitude 0.05): in its first thousand steps FP32 rounding
+    # loses mass systematically, step after step, which the feedback must
+    # anticipate to hold the drift within 1e-10
+    n = 128
+    ic = mb.ic_generate((n, n, n), 0.2484214642537962, 0.05, False, 1046)
+    p = mb.make_params(n, n, n, 0.005, kappa=0.7051460773138722, precision="fp32", mass_correct=every)
+    with mb.CHSim(p) as sim:
+        sim.set_field(ic)
+        m0 = sim.reduce()["mass"]
+        for _ in range(4):
+            sim.step(250)
+            r = sim.reduce()
+            assert abs(r["mass"] - m0) / abs(m0) <= 1e-10, r
+
+
 def test_diagnostics_match_oracle(oracle):
     dims = (64, 40, 24)
     c = oracle.ic(dims, 0.2, 0.3, False, 6)
