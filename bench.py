@@ -265,6 +265,61 @@ def run_batch(mb, torch, dev, steps, sampler):
             "l2": "fields (about 1.5 GB) larger than L2"}
 
 
+def run_precision(mb, dev, steps, n=512, seed=42, every=250):
+    """Precision study (C3): the off-critical quench at n^3, c0 = 0.3 plus
+    Gaussian noise sigma 0.02, dt 0.005, M 1, kappa 1.5, stepped in FP32
+    (FP64 reductions, mass feedback) and in FP64 -- the drop-in path, which
+    is bit-identical to the reference build and so serves as the FP64 oracle
+    at a size the CPU build cannot run in minutes.  Reports the FP32 max-norm
+    error at step 100, the mass drift of both, the free energy of both every
+    `every` steps, and the structure-factor peak wavenumber of both at the
+    end."""
+    import numpy as np
+    ic = mb.ic_generate((n, n, n), 0.3, 0.02, True, seed)
+    kw = dict(kappa=1.5, M=1.0)
+    t0 = time.perf_counter()
+    sims = {prec: mb.CHSim(mb.make_params(n, n, n, DT, precision=prec, **kw), dev) for prec in ("fp64", "fp32")}
+    out = {"workload": f"{n}^3, c0 = 0.3 + N(0, 0.02^2) seed {seed}, dt 0.005, M 1, kappa 1.5, {steps} steps; "
+                       "FP32 = FP32 field, FP64 reductions, mass feedback every 4th step; FP64 = the drop-in path"}
+    try:
+        for sim in sims.values():
+            sim.set_field(ic)
+        del ic
+        r0 = {p: s.reduce() for p, s in sims.items()}
+        curve = {p: [(0, r0[p]["energy"])] for p in sims}
+        done = 0
+        marks = sorted(set([min(100, steps)] + list(range(every, steps + 1, every)) + [steps]))
+        for m in marks:
+            for s in sims.values():
+                s.step(m - done)
+            done = m
+            r = {p: s.reduce() for p, s in sims.items()}
+            for p in sims:
+                curve[p].append((m, r[p]["energy"]))
+            if m == min(100, steps):
+                a = sims["fp64"].get_field()
+                b = sims["fp32"].get_field()
+                out["maxnorm_fp32_vs_fp64_at_step"] = m
+                out["maxnorm_fp32_vs_fp64"] = float(np.max(np.abs(a - b)))
+                del a, b
+        r1 = {p: s.reduce() for p, s in sims.items()}
+        for p in sims:
+            out[f"mass_drift_rel_{p}"] = abs(r1[p]["mass"] - r0[p]["mass"]) / abs(r0[p]["mass"])
+        out["mass_fp32_minus_fp64_rel"] = abs(r1["fp32"]["mass"] - r1["fp64"]["mass"]) / abs(r1["fp64"]["mass"])
+        out["energy"] = {p: [[m, e] for m, e in curve[p]] for p in sims}
+        out["energy_rel_diff_max"] = max(abs(e32 - e64) / abs(e64) for (_, e32), (_, e64)
+                                         in zip(curve["fp32"], curve["fp64"]))
+        out["energy_decays"] = {p: all(b[1] <= a[1] for a, b in zip(curve[p], curve[p][1:])) for p in sims}
+        k1 = {p: s.structure_factor(64)[2] for p, s in sims.items()}
+        out["sk_peak_k1"] = k1
+        out["sk_peak_rel_diff"] = abs(k1["fp32"] - k1["fp64"]) / abs(k1["fp64"])
+        out["wall_s"] = time.perf_counter() - t0
+    finally:
+        for s in sims.values():
+            s.close()
+    return out
+
+
 def run_serve(mb, dev, window_s, seed=11, rate=20.0):
     """Served stream: Poisson arrivals at `rate` jobs/s for `window_s` seconds, then drain."""
     import numpy as np
@@ -413,6 +468,7 @@ def run_ours(args, rank, world, local_rank):
     models = (run_models(mb, torch, dev, min(args.steps, 20), max(args.warmup, 3), flush, sampler, load_peaks()[0])
               if args.model_steps else None)
     batch = run_batch(mb, torch, dev, args.batch_steps, sampler) if args.batch_steps > 0 else None
+    precision = run_precision(mb, dev, args.precision_steps) if args.precision_steps > 0 else None
     clocks = sampler.summary()
     serve = None
     if args.serve_seconds > 0:
@@ -473,6 +529,7 @@ def run_ours(args, rank, world, local_rank):
         "tiling": out["fp64"]["tiling"],
         "batch": batch,
         "serve": serve,
+        "precision": precision,
         "models": models,
         "cpu_baseline": cpu,
         "clocks": clocks,
@@ -557,6 +614,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=1000, help="steps of the batched sweep (0: skip)")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrival window of the served stream (0: skip)")
     ap.add_argument("--serve-runs", type=int, default=3, help="runs of the served stream (the median is reported)")
+    ap.add_argument("--precision-steps", type=int, default=2000,
+                    help="steps of the 512^3 FP32-vs-FP64 precision study (0: skip)")
     ap.add_argument("--model-steps", type=int, default=1, help="time the variable-mobility models (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
