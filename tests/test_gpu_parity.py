@@ -127,6 +127,31 @@ def test_c1_2d_256_fp64_matches_reference_after_100_steps(oracle):
     assert np.array_equal(got, want)
 
 
+def test_c1_2d_256_fp64_full_run_matches_oracle(oracle):
+    # configuration C1 at full length: 10,000 steps with mass and free energy
+    # logged every 1,000.  Spinodal decomposition is chaotic, so a field that
+    # is still bit-identical after 10,000 steps has matched every operation.
+    dims = (256, 256, 1)
+    c = oracle.ic(dims, 0.0, 0.2, False, 42)
+    p = mb.make_params(256, 256, 1, 0.01)
+    with mb.CHSim(p) as sim:
+        sim.set_field(c)
+        m0 = sim.reduce()["mass"]
+        scale = float(np.abs(c).sum())
+        energy = [sim.reduce()["energy"]]
+        for _ in range(10):
+            sim.step(1000)
+            c = oracle.run(c, dims, (1, 1, 1), 0.01, 1.0, 1.0, 1000)
+            got = sim.get_field()
+            assert np.array_equal(got, c), np.abs(got - c).max()
+            r, want = sim.reduce(), oracle.reduce(c, dims)
+            assert abs(r["mass"] - want["mass"]) <= 1e-12 * scale
+            assert abs(r["energy"] - want["energy"]) <= 1e-12 * abs(want["energy"])
+            assert abs(r["mass"] - m0) <= 1e-12 * scale  # c0 = 0: drift relative to sum |c(0)|
+            energy.append(r["energy"])
+    assert all(b <= a for a, b in zip(energy, energy[1:])), energy
+
+
 def test_c2_3d_128_fp64_matches_oracle(oracle):
     dims = (128, 128, 128)
     ic = oracle.ic(dims, 0.0, 0.1, False, 42)
