@@ -266,6 +266,17 @@ __device__ __forceinline__ long long strip_mass(float o0, float o1, float o2, fl
     return __double2ll_rn((x + y) * (double)kMassScale);
 }
 
+// Does the nudge window [w0, w0 + |cnt|) (wrapping at nsites) reach the row
+// of sites [rs, rs + len)?  Asked only in planes the window reaches, so that
+// only the threads of the rows it covers take the out-of-line nudge.
+__device__ __forceinline__ bool window_reaches(long long rs, long long len, long long w0, long long cnt,
+                                               long long nsites)
+{
+    const long long w1 = w0 + (cnt < 0 ? -cnt : cnt);
+    if (rs < w1 && rs + len > w0) return true;
+    return w1 > nsites && rs < w1 - nsites;
+}
+
 // Adds the mass nudge to the elements of a thread's 8-float strip whose sites
 // lie in the nudge window (sites of element e: site0 + e for e < 4, site0 +
 // offB + e - 4 for the second half).  Called only for planes the window
@@ -660,7 +671,8 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
 #pragma unroll
                         for (int k = 0; k < 4; ++k) out.p[k] = fma2(lp[k], dt2, cp.p[k]);
                         if constexpr (MASS) {
-                            if (hit) {
+                            if (hit && window_reaches((long long)(zoff + rowoff - xA), nx, head->nudge_begin,
+                                                      head->nudge_count, (long long)pstride * nz)) {
                                 float o[8];
 #pragma unroll
                                 for (int e = 0; e < 8; ++e) o[e] = out.get(e);
@@ -702,7 +714,8 @@ __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step
                         }
                         if constexpr (sizeof(T) == 4) {
                             if constexpr (MASS) {
-                                if (hit) {
+                                if (hit && window_reaches((long long)(zoff + rowoff - xA), nx, head->nudge_begin,
+                                                          head->nudge_count, (long long)pstride * nz)) {
                                     float t[8];
 #pragma unroll
                                     for (int e = 0; e < 8; ++e) t[e] = o[e];

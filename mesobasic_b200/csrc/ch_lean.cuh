@@ -258,7 +258,8 @@ __global__ void __launch_bounds__(kMaxBlock, 1) ch_lean_kernel(StepArgs a)
                     for (int k = 0; k < 4; ++k) out.p[k] = fma2(lp[k], dt2, cp.p[k]);
                     const size_t zoff = (size_t)zo * pstride;
                     if constexpr (MASS) {
-                        if (hit) {
+                        if (hit && window_reaches((long long)zoff + site_row - xA, NXC, head->nudge_begin,
+                                                  head->nudge_count, (long long)pstride * nz)) {
                             float o[8];
 #pragma unroll
                             for (int e = 0; e < 8; ++e) o[e] = out.get(e);
