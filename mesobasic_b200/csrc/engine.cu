@@ -621,6 +621,7 @@ Engine::~Engine()
     cudaFreeHost(h_state_);
     free_graveyard();
     for (cudaStream_t st : aux_) cudaStreamDestroy(st);
+    if (side) cudaStreamDestroy(side);
     for (cudaEvent_t ev : aux_ev_) cudaEventDestroy(ev);
     if (fork_ev_) cudaEventDestroy(fork_ev_);
     if (stream) cudaStreamDestroy(stream);
@@ -1098,8 +1099,13 @@ int Engine::sync(long long timeout_us)
 int Engine::read_state(Job* j, JobDev* out)
 {
     MG_CUDA(cudaSetDevice(device));
-    MG_CUDA(cudaMemcpyAsync(h_state_, d_jobs_ + j->slot, sizeof(JobDev), cudaMemcpyDeviceToHost, stream));
-    MG_CUDA(cudaStreamSynchronize(stream));
+    return read_state_on(j, out, stream);
+}
+
+int Engine::read_state_on(Job* j, JobDev* out, cudaStream_t st)
+{
+    MG_CUDA(cudaMemcpyAsync(h_state_, d_jobs_ + j->slot, sizeof(JobDev), cudaMemcpyDeviceToHost, st));
+    MG_CUDA(cudaStreamSynchronize(st));
     *out = *h_state_;
     return MG_OK;
 }
@@ -1159,16 +1165,37 @@ int Engine::download(Job* j, double* host)
 {
     if (!host) return fail(MG_EINVAL, "null field");
     MG_TRY(sync(-1));
-    MG_TRY(read_state(j, h_state_));
+    return download_on(j, host, stream);
+}
+
+int Engine::ensure_side()
+{
+    if (!side) MG_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    return MG_OK;
+}
+
+int Engine::download_finished(Job* j, double* host)
+{
+    if (!host) return fail(MG_EINVAL, "null field");
+    MG_CUDA(cudaSetDevice(device));
+    MG_TRY(ensure_side());
+    return download_on(j, host, side);
+}
+
+// copies the job's current field to the host through stream `st` and waits
+// for that stream only
+int Engine::download_on(Job* j, double* host, cudaStream_t st)
+{
+    MG_TRY(read_state_on(j, h_state_, st));
     const void* cur = j->buf[h_state_->step & 1];
     if (j->g.es == 8) {
-        MG_CUDA(cudaMemcpyAsync(host, cur, j->g.n * 8, cudaMemcpyDeviceToHost, stream));
+        MG_CUDA(cudaMemcpyAsync(host, cur, j->g.n * 8, cudaMemcpyDeviceToHost, st));
     } else {
         MG_TRY(ensure_stage(j->g.n));
-        ch_convert<float, double><<<4 * info.sms, 256, 0, stream>>>(static_cast<const float*>(cur), d_stage_, j->g.n);
-        MG_CUDA(cudaMemcpyAsync(host, d_stage_, j->g.n * 8, cudaMemcpyDeviceToHost, stream));
+        ch_convert<float, double><<<4 * info.sms, 256, 0, st>>>(static_cast<const float*>(cur), d_stage_, j->g.n);
+        MG_CUDA(cudaMemcpyAsync(host, d_stage_, j->g.n * 8, cudaMemcpyDeviceToHost, st));
     }
-    MG_CUDA(cudaStreamSynchronize(stream));
+    MG_CUDA(cudaStreamSynchronize(st));
     return MG_OK;
 }
 
@@ -1185,18 +1212,31 @@ int Engine::diagnostics(Job* j, mg_ch_stats* out)
 {
     if (!out) return fail(MG_EINVAL, "null stats");
     MG_TRY(sync(-1));
+    return diagnostics_on(j, out, stream);
+}
+
+int Engine::diagnostics_finished(Job* j, mg_ch_stats* out)
+{
+    if (!out) return fail(MG_EINVAL, "null stats");
+    MG_CUDA(cudaSetDevice(device));
+    MG_TRY(ensure_side());
+    return diagnostics_on(j, out, side);
+}
+
+int Engine::diagnostics_on(Job* j, mg_ch_stats* out, cudaStream_t st)
+{
     const Geometry& g = j->g;
     if (g.es == 8)
-        ch_diag_partial<double><<<kDiagBlocks, kDiagThreads, 0, stream>>>(d_jobs_ + j->slot, g.lsx, g.lsy, g.lsz,
-                                                                           d_diag_part_, d_diag_max_, d_diag_bad_);
+        ch_diag_partial<double><<<kDiagBlocks, kDiagThreads, 0, st>>>(d_jobs_ + j->slot, g.lsx, g.lsy, g.lsz,
+                                                                       d_diag_part_, d_diag_max_, d_diag_bad_);
     else
-        ch_diag_partial<float><<<kDiagBlocks, kDiagThreads, 0, stream>>>(d_jobs_ + j->slot, g.lsx, g.lsy, g.lsz,
-                                                                          d_diag_part_, d_diag_max_, d_diag_bad_);
-    ch_diag_final<<<1, 256, 0, stream>>>(d_diag_part_, d_diag_max_, d_diag_bad_, kDiagBlocks, g.lsx * g.lsy * g.lsz,
-                                         d_diag_);
+        ch_diag_partial<float><<<kDiagBlocks, kDiagThreads, 0, st>>>(d_jobs_ + j->slot, g.lsx, g.lsy, g.lsz,
+                                                                      d_diag_part_, d_diag_max_, d_diag_bad_);
+    ch_diag_final<<<1, 256, 0, st>>>(d_diag_part_, d_diag_max_, d_diag_bad_, kDiagBlocks, g.lsx * g.lsy * g.lsz,
+                                     d_diag_);
     MG_CUDA(cudaGetLastError());
-    MG_CUDA(cudaMemcpyAsync(h_diag_, d_diag_, sizeof(Diag), cudaMemcpyDeviceToHost, stream));
-    MG_TRY(read_state(j, h_state_));  // syncs the stream
+    MG_CUDA(cudaMemcpyAsync(h_diag_, d_diag_, sizeof(Diag), cudaMemcpyDeviceToHost, st));
+    MG_TRY(read_state_on(j, h_state_, st));  // syncs the stream
     out->mass = h_diag_->mass;
     out->energy = h_diag_->energy;
     out->abs_mass = h_diag_->abs_mass;

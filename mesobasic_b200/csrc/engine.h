@@ -107,6 +107,12 @@ class Engine {
     int upload(Job* j, const double* host, long long target);  // resets step
     int download(Job* j, double* host);                         // syncs
     int diagnostics(Job* j, mg_ch_stats* out);                  // syncs
+    // The same for a job that has reached its step target, on a side stream
+    // and without waiting for the steps in flight on the engine stream: the
+    // kernels skip a finished job's items, so its field and slot stay as
+    // they are.  One thread at a time (they share the staging buffers).
+    int download_finished(Job* j, double* host);
+    int diagnostics_finished(Job* j, mg_ch_stats* out);
     // appends the job's current field as legacy VTK, formatted on the GPU (vtk_device.cu)
     int write_vtk(Job* j, const char* path, const char* tag, int iskip, int jskip, int kskip);
     int structure_factor(Job* j, int nbins, double* k, double* S, double* k1);
@@ -130,6 +136,7 @@ class Engine {
     int batch_threads = 320;
     int batch_planes = 128;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;  // created on first use (download_finished)
     DevInfo info;
     std::vector<Job*> jobs;
 
@@ -158,6 +165,10 @@ class Engine {
     int graph_for(int k, cudaGraphExec_t* out);
     void drop_graphs();
     int to_double(Job* j, double* d_dst);   // current field -> device doubles
+    int download_on(Job* j, double* host, cudaStream_t st);
+    int diagnostics_on(Job* j, mg_ch_stats* out, cudaStream_t st);
+    int read_state_on(Job* j, JobDev* out, cudaStream_t st);
+    int ensure_side();
     int ensure_stage(size_t n);
 
     int capacity_ = 0;

@@ -10,7 +10,9 @@
 //      that reaches its step count stops on the device (its tiles skip), so
 //      ticks keep one length and one captured graph per job set;
 //   3. retires jobs that reached their step count: downloads the field and
-//      diagnostics, frees their memory, records the latency.
+//      diagnostics on a side stream while the next tick runs (their tiles
+//      skip, so their fields do not change), frees their memory, records
+//      the latency.
 // Per-job arithmetic does not depend on which other jobs share a launch:
 // each job's decomposition and reduction trees depend on its own shape only.
 #include <algorithm>
@@ -120,9 +122,12 @@ void mg_server::retire(ServerJob* sj, bool ok, const char* why)
     if (ok) {
         sj->result_n = (size_t)sj->p.nx * sj->p.ny * sj->p.nz;
         sj->result.reset(new (std::nothrow) double[sj->result_n]);
-        int rc = sj->result ? eng.download(sj->job, sj->result.get()) : fail(MG_ENOMEM, "host allocation failed");
+        // the job has reached its step count: its field is read on the
+        // engine's side stream while the next tick runs
+        int rc = sj->result ? eng.download_finished(sj->job, sj->result.get())
+                            : fail(MG_ENOMEM, "host allocation failed");
         if (rc == MG_OK) {
-            rc = eng.diagnostics(sj->job, &sj->stats);
+            rc = eng.diagnostics_finished(sj->job, &sj->stats);
             if (rc == MG_ENONFINITE) rc = MG_OK;  // reported in stats.nonfinite
         }
         if (rc != MG_OK) {
@@ -158,6 +163,9 @@ static double seconds_since(Clock::time_point t0)
 void mg_server::run()
 {
     cudaSetDevice(eng.device);
+    // jobs that reached their step count in the last tick: retired (field
+    // and diagnostics read on a side stream) while the next tick runs
+    std::vector<ServerJob*> finished;
     for (;;) {
         {
             std::unique_lock<std::mutex> lock(mu);
@@ -173,27 +181,34 @@ void mg_server::run()
             }
         }
         const long long k = steps_per_tick;
+        // steps only when some admitted job still has steps to take
+        const bool stepping = running.size() > finished.size();
         const auto t0 = Clock::now();
-        int rc = eng.enqueue_steps((int)k);
-        if (rc == MG_OK) rc = eng.sync(600LL * 1000 * 1000);
+        int rc = stepping ? eng.enqueue_steps((int)k) : MG_OK;
+        const auto t1 = Clock::now();
+        for (ServerJob* sj : finished) retire(sj, true, nullptr);
+        finished.clear();
+        const double rs = seconds_since(t1);
+        if (stepping && rc == MG_OK) rc = eng.sync(600LL * 1000 * 1000);
         {
             std::lock_guard<std::mutex> lock(mu);
-            step_s += seconds_since(t0);
-            ++ticks;
+            retire_s += rs;
+            if (stepping) {
+                step_s += seconds_since(t0);
+                ++ticks;
+            }
         }
-        const auto t1 = Clock::now();
         std::vector<ServerJob*> snapshot = running;
         if (rc != MG_OK) {
             const std::string why = mg::last_error();
             for (ServerJob* sj : snapshot) retire(sj, false, why.c_str());
             continue;
         }
+        if (!stepping) continue;
         for (ServerJob* sj : snapshot) {
             sj->done_steps = std::min(sj->nsteps, sj->done_steps + k);
-            if (sj->done_steps >= sj->nsteps) retire(sj, true, nullptr);
+            if (sj->done_steps >= sj->nsteps) finished.push_back(sj);
         }
-        std::lock_guard<std::mutex> lock(mu);
-        retire_s += seconds_since(t1);
     }
 }
 
