@@ -258,7 +258,7 @@ def run_batch(mb, torch, dev, steps, sampler):
             "value": sites * steps / (ms * 1e-3) / 1e9, "unit": "GLUPS", "precision": "fp32 (mass feedback every 4th step)",
             "launches_per_step": info["launches_per_step"], "persistent_ctas": info["ctas"],
             "max_mass_drift_per_site": drift,
-            "mass_drift_note": "max over jobs of |M(1004) - M(4)| / sites, FP64 sums of the stored fields; the "
+            "mass_drift_note": f"max over jobs of |M({4 + steps}) - M(4)| / sites, FP64 sums of the stored fields; the "
                                "feedback measures and corrects the mass after every 4th step",
             "workload": "64 cubic jobs, edges uniform from {64,96,128,160,192}, c0 U[-0.4,0.4], kappa U[0.5,2], "
                         "noise amplitude 0.05, seeds 1000+j (draws seed 7), dt 0.005",
