@@ -106,7 +106,7 @@ int run(int argc, char** argv)
     std::vector<std::unique_ptr<PFApp>> apps;
     for (const std::string& sec : in.section_names()) {
         if (in((sec + "app").c_str(), "false") != "true") continue;
-        if (sec != "PFApp/") throw std::invalid_argument("section '" + sec + "' is not an application of this build");
+        if (sec != "PFApp/") throw std::invalid_argument("section '" + sec + "' is not an application meso_b200 runs");
         apps.emplace_back(new PFApp(in));
     }
     for (auto& a : apps) {

@@ -17,7 +17,7 @@ PFBaseClass* PFBaseClass::PFFactory(const CommonParams& p, const InputFile& in)
     if (type == "SIPS" || type == "SIPSGPU") return new SIPSGPU(p, in);
     if (type == "SIPSternary" || type == "SIPSternaryGPU") return new SIPSternaryGPU(p, in);
     throw std::invalid_argument("PFApp/type '" + type +
-                                "' is not provided by this build (available: CHBasic, CHBasicGPU, TIPSphil, "
+                                "' is not provided by meso_b200 (available: CHBasic, CHBasicGPU, TIPSphil, "
                                 "TIPSphilGPU, TIPSbathPHIL, TIPSbathPHILGPU, SIPS, SIPSGPU, SIPSternary, "
                                 "SIPSternaryGPU)");
 }

@@ -1,5 +1,5 @@
 /*
- * TEST INFRASTRUCTURE ONLY: the checker for the GPU path (see ch_oracle.h).
+ * TEST INFRASTRUCTURE ONLY: the oracle for the GPU path (see ch_oracle.h).
  * Compiled with -ffp-contract=off so that every product and sum is rounded
  * separately, in the order written, as in the reference's x86-64 build.
  */

@@ -1,7 +1,7 @@
 /*
  * TEST INFRASTRUCTURE ONLY.  Plain-C restatement of the reference's
  * Cahn-Hilliard step and its seeded initial condition, used by the tests,
- * the smoke check and the CPU-baseline leg of the benchmark as the checker.
+ * the smoke check and the CPU-baseline leg of the benchmark as the oracle.
  * Nothing in the product path links or calls it.
  *
  * Layout: dense, x fastest, no ghost nodes: index x + nx*(y + ny*z).

@@ -1,4 +1,4 @@
-"""TEST INFRASTRUCTURE ONLY: Python access to the checkers.
+"""TEST INFRASTRUCTURE ONLY: Python access to the oracles.
 
 * ``libchoracle.so``: the plain-C restatement of the reference's CH step
   (ch_oracle.c), built by ``make -C oracle``.

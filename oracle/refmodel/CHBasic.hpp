@@ -1,7 +1,7 @@
 // Test infrastructure: the plain Cahn-Hilliard model for the reference CPU
 // build.  It is compiled together with the reference's own sources (SfieldFD,
 // Rand, PFBaseClass, PFApp, MesoExecute) into oracle/_ref/ and is the
-// checker the GPU path is compared against; nothing in the product links it.
+// oracle the GPU path is compared against; nothing in the product links it.
 //
 // The reference factory names "CHBasic" as its default type but the class
 // is absent (PFBaseClass.cpp:9,34,40).  This class fills that slot, following

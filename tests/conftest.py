@@ -1,5 +1,5 @@
 """Shared test setup: the `gpu` marker, paths, and fixtures that load the
-golden vectors and the checkers (oracle/)."""
+golden vectors and the oracles (oracle/)."""
 import json
 import os
 import sys

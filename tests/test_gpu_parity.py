@@ -1,4 +1,4 @@
-"""GPU path against the checkers, through the C ABI.
+"""GPU path against the oracles, through the C ABI.
 
 FP64: bit-identical to the reference build (golden vectors) and to the C
 restatement at every tiling, boundary condition and spacing.  FP32: within
@@ -179,7 +179,7 @@ def test_constant_field_fixed_point_and_mass():
 
 
 def test_fp32_within_tolerance_of_fp64_after_100_steps(oracle):
-    # north-star budget: <= 1e-4 max-norm after 100 steps vs the FP64 oracle
+    # the FP32 accuracy budget: <= 1e-4 max-norm after 100 steps vs the FP64 oracle
     dims = (64, 64, 64)
     ic = oracle.ic(dims, 0.3, 0.02, True, 42)
     want = oracle.run(ic, dims, (1, 1, 1), 0.005, 1.0, 1.5, 100)

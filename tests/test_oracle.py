@@ -1,4 +1,4 @@
-"""The checker itself: the C restatement (oracle/ch_oracle.c) pinned to the
+"""The oracle itself: the C restatement (oracle/ch_oracle.c) pinned to the
 golden vectors written by the reference CPU build, to the reference build
 itself when it is present, and to known answers from mathematics."""
 import json
