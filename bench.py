@@ -38,6 +38,10 @@ CONFIG = {"workload": "3-D Cahn-Hilliard 256^3 explicit step, dt 0.005, M 1, kap
                 "so that no dirty line of the flush is left to write back inside the timed step",
           "parallelism": "replicas (one independent simulation per GPU)"}
 METRIC = "GLUPS & % HBM roofline (FP32 vs FP64)"
+# DRAM traffic per launch is read from the committed ncu summaries (one
+# capture of the same kernel and tiling), not measured inside this run
+TRAFFIC_SOURCE = {"fp64": "ncu capture in profiles/ncu_ch_step_fp64_256.md (same kernel and tiling)",
+                  "fp32": "ncu capture in profiles/ncu_ch_step_fp32_256.md (same kernel and tiling)"}
 
 
 def load_peaks():
@@ -235,7 +239,8 @@ def run_batch(mb, torch, dev, steps, sampler):
         # corrected it (every 4th step)
         b.step(4)
         b.sync()
-        m0 = [b.reduce(j)["mass"] for j in range(len(jobs))]
+        r0 = [b.reduce(j) for j in range(len(jobs))]
+        m0 = [r["mass"] for r in r0]
         ext = torch.cuda.ExternalStream(b.stream, device=f"cuda:{dev}")
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -250,16 +255,18 @@ def run_batch(mb, torch, dev, steps, sampler):
         info = b.info()
         sites_j = [d[0] * d[1] * d[2] for d, _, _, _ in jobs]
         # mass drift relative to the mass scale sum|c| ~ N*|c0|+noise: per site
-        drift = max(abs(b.reduce(j)["mass"] - m0[j]) / sites_j[j] for j in range(len(jobs)))
+        m1 = [b.reduce(j)["mass"] for j in range(len(jobs))]
+        drift = max(abs(m1[j] - m0[j]) / sites_j[j] for j in range(len(jobs)))
+        drift_rel = max(abs(m1[j] - m0[j]) / r0[j]["abs_mass"] for j in range(len(jobs)))
     finally:
         b.close()
     sites = float(sum(d[0] * d[1] * d[2] for d, _, _, _ in jobs))
     return {"jobs": len(jobs), "sites": sites, "steps": steps, "ms": ms,
-            "value": sites * steps / (ms * 1e-3) / 1e9, "unit": "GLUPS", "precision": "fp32 (mass feedback every 4th step)",
+            "value": sites * steps / (ms * 1e-3) / 1e9, "unit": "GLUPS", "precision": f"fp32 (mass feedback every {mb.MASS_EVERY} step(s))",
             "launches_per_step": info["launches_per_step"], "persistent_ctas": info["ctas"],
-            "max_mass_drift_per_site": drift,
+            "max_mass_drift_per_site": drift, "max_mass_drift_rel": drift_rel,
             "mass_drift_note": f"max over jobs of |M({4 + steps}) - M(4)| / sites, FP64 sums of the stored fields; the "
-                               "feedback measures and corrects the mass after every 4th step",
+                               f"feedback measures and corrects the mass after every {mb.MASS_EVERY} step(s)",
             "workload": "64 cubic jobs, edges uniform from {64,96,128,160,192}, c0 U[-0.4,0.4], kappa U[0.5,2], "
                         "noise amplitude 0.05, seeds 1000+j (draws seed 7), dt 0.005",
             "l2": "fields (about 1.5 GB) larger than L2"}
@@ -280,7 +287,7 @@ def run_precision(mb, dev, steps, n=512, seed=42, every=250):
     t0 = time.perf_counter()
     sims = {prec: mb.CHSim(mb.make_params(n, n, n, DT, precision=prec, **kw), dev) for prec in ("fp64", "fp32")}
     out = {"workload": f"{n}^3, c0 = 0.3 + N(0, 0.02^2) seed {seed}, dt 0.005, M 1, kappa 1.5, {steps} steps; "
-                       "FP32 = FP32 field, FP64 reductions, mass feedback every 4th step; FP64 = the drop-in path"}
+                       f"FP32 = FP32 field, FP64 reductions, mass feedback every {mb.MASS_EVERY} step(s); FP64 = the drop-in path"}
     try:
         for sim in sims.values():
             sim.set_field(ic)
@@ -516,26 +523,44 @@ def run_ours(args, rank, world, local_rank):
     if batch:
         batch["roofline_frac"] = batch["value"] * 8 / peak  # GB/s of algorithmic bytes / peak
     cpu = cpu_baseline_sample()
+    detail = {"fp64": out["fp64"], "fp32": out["fp32"], "batch": batch, "serve": serve, "precision": precision,
+              "models": models, "cpu_baseline": cpu, "clocks": clocks}
+    if args.detail:
+        with open(args.detail, "w") as f:
+            json.dump(detail, f, indent=1)
+    r64, r32 = out["fp64"]["roofline"], out["fp32"]["roofline"]
     line = {
         "metric": METRIC, "value": out["fp64"]["value"], "unit": "GLUPS", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["fp64"]["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": dict(CONFIG, precision="fp64 drop-in (bit-identical to the reference build)"),
-        "roofline": out["fp64"]["roofline"],
-        "e2e": out["fp64"]["e2e"],
-        "fp32": {k: out["fp32"][k] for k in ("value", "ms_per_step", "roofline", "e2e", "tiling")}
-                | {"dtype": "f32 field, f64 reductions, mass feedback every 4th step",
-                   "speedup_vs_fp64": out["fp32"]["value"] / out["fp64"]["value"]},
-        "tiling": out["fp64"]["tiling"],
-        "batch": batch,
-        "serve": serve,
-        "precision": precision,
-        "models": models,
+        "roofline": {k: r64[k] for k in ("bound", "achieved", "peak", "unit", "frac", "traffic")}
+                    | {"traffic_source": TRAFFIC_SOURCE["fp64"], "peak_kind": r64["peak_kind"]},
+        "e2e": {k: out["fp64"]["e2e"][k] for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step")},
+        "fp32": {"value": out["fp32"]["value"], "ms_per_step": out["fp32"]["ms_per_step"],
+                 "frac": r32["frac"], "achieved_gbs": r32["achieved"], "traffic": r32["traffic"],
+                 "speedup_vs_fp64": out["fp32"]["value"] / out["fp64"]["value"],
+                 "e2e": out["fp32"]["e2e"]["value"],
+                 "mass_correct": mb.MASS_EVERY},
+        "batch": None if not batch else {
+            "value": batch["value"], "roofline_frac": batch["roofline_frac"], "jobs": batch["jobs"],
+            "steps": batch["steps"], "launches_per_step": batch["launches_per_step"],
+            "max_mass_drift_per_site": batch["max_mass_drift_per_site"],
+            "max_mass_drift_rel": batch["max_mass_drift_rel"]},
+        "serve": None if not serve else {
+            "sims_per_hour": serve["sims_per_hour"], "p50_ms": serve["p50_ms"], "p99_ms": serve["p99_ms"],
+            "glups": serve["glups"], "runs": len(serve["runs"]), "reported": serve["reported"],
+            "saturated": serve.get("saturated")},
+        "precision": None if not precision else {
+            k: precision.get(k) for k in ("maxnorm_fp32_vs_fp64", "mass_drift_rel_fp32", "mass_drift_rel_fp64",
+                                          "sk_peak_rel_diff", "energy_rel_diff_max")},
+        "models": None if not models else {k: round(v["value"], 2) for k, v in models.items() if isinstance(v, dict)},
         "cpu_baseline": cpu,
-        "clocks": clocks,
+        "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         "gpu_launches": args.steps,
-        "gpu_launches_note": "one fused ch_step_kernel launch per timed step in the fp64 region (the headline); "
-                             "the fp32 region likewise; the batch region one launch per precision class and step",
+        "notes": "fp64 = headline (one fused step launch per timed step, L2 flushed between steps); fp32 = FP32 "
+                 "field with FP64 mass feedback; batch = C4 64 jobs; serve = C5 stream, median run; "
+                 "per-leg detail in the --detail file",
     }
     print(json.dumps(line), flush=True)
     if dist:
@@ -617,6 +642,7 @@ def main():
     ap.add_argument("--precision-steps", type=int, default=2000,
                     help="steps of the 512^3 FP32-vs-FP64 precision study (0: skip)")
     ap.add_argument("--model-steps", type=int, default=1, help="time the variable-mobility models (0: skip)")
+    ap.add_argument("--detail", default=None, help="write every leg's full record to this JSON file")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

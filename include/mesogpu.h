@@ -344,11 +344,14 @@ void mg_server_destroy(mg_server_t* s);
  * holds only a borrowed device pointer and no handle.  Its scratch is one
  * fixed device array of about 256 KB per process, which bounds the field to
  * at most 4096 planes (nz for 3-D fields, ny for 2-D ones); larger fields
- * give MG_EINVAL (use mg_ch_reduce).  The first call on a device looks up
- * that array's address and should come before any stream capture there.
+ * give MG_EINVAL (use mg_ch_reduce).  Every call looks up that array's
+ * address on `device`; the first call on a device also loads the library's
+ * device code there and should come before any stream capture there.
  * Calls that overlap in time on one device share the array and race: issue
- * them one at a time.  Sums are compensated FP64 in a fixed order; they
- * agree with mg_ch_reduce to rounding (the two sum in different orders). */
+ * them one at a time.  After MG_ETIMEOUT the kernel is still on `stream`:
+ * synchronise that stream before calling again on the device.  Sums are
+ * compensated FP64 in a fixed order; they agree with mg_ch_reduce to
+ * rounding (the two sum in different orders). */
 int mg_field_stats_noalloc(const void* field_dev, const mg_ch_params* params, int device, void* stream,
                            long long timeout_us, mg_ch_stats* out);
 

@@ -18,15 +18,20 @@
 // nz == 1), so fields with more than kNoAllocMaxPlanes planes are rejected
 // with MG_EINVAL.
 //
-// Set-up: the first call on a device looks up the array's device address
-// (cudaGetSymbolAddress, with that device current) and keeps it for later
-// calls; make that first call before any stream capture on the device.
-// Every call clears the completion counter (cudaMemsetAsync on the caller's
-// stream) before its launch.
+// Set-up: every call looks up the array's device address
+// (cudaGetSymbolAddress, with that device current), so a device reset
+// between calls cannot leave a stale address behind.  The first lookup on a
+// device loads this library's device code there: make that first call
+// before any stream capture on the device.  Every call clears the
+// completion counter (cudaMemsetAsync on the caller's stream) before its
+// launch.
 //
 // Concurrency: all calls on one device share the one scratch array, so calls
 // that overlap in time -- from several host threads, or on several streams
-// -- race and may return wrong numbers.  Issue them one at a time.
+// -- race and may return wrong numbers.  Issue them one at a time.  A call
+// that returns MG_ETIMEOUT leaves its kernel queued or running on the
+// caller's stream: synchronise that stream before the next call on the
+// device, or the next call races it.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -154,24 +159,19 @@ __global__ void __launch_bounds__(kNoAllocThreads)
     }
 }
 
-// device address of g_noalloc_scratch, looked up once per device
+// device address of g_noalloc_scratch on the current device, looked up on
+// every call (cheap once the module is loaded)
 unsigned char* scratch_address(int device, int* rc)
 {
-    static std::mutex mu;
-    static unsigned char* addr[kNoAllocMaxDevices] = {};
-    std::lock_guard<std::mutex> lk(mu);
-    if (!addr[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            *rc = fail(MG_ECUDA, "cudaGetSymbolAddress of the no-allocation scratch failed on device %d: %s", device,
-                       cudaGetErrorString(e));
-            return nullptr;
-        }
-        addr[device] = static_cast<unsigned char*>(p);
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        *rc = fail(MG_ECUDA, "cudaGetSymbolAddress of the no-allocation scratch failed on device %d: %s", device,
+                   cudaGetErrorString(e));
+        return nullptr;
     }
     *rc = MG_OK;
-    return addr[device];
+    return static_cast<unsigned char*>(p);
 }
 
 int field_stats_noalloc(const void* field, const mg_ch_params* p, int device, cudaStream_t stream,
@@ -222,7 +222,11 @@ int field_stats_noalloc(const void* field, const mg_ch_params* p, int device, cu
         if (timeout_us >= 0) {
             const auto us =
                 std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0).count();
-            if (us > timeout_us) return fail(MG_ETIMEOUT, "reduction not finished after %lld us", timeout_us);
+            if (us > timeout_us)
+                return fail(MG_ETIMEOUT,
+                            "reduction not finished after %lld us; its kernel is still on the stream: synchronise "
+                            "the stream before the next call",
+                            timeout_us);
         }
         std::this_thread::sleep_for(std::chrono::microseconds(20));
     }

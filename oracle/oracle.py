@@ -25,7 +25,19 @@ ORACLE_SO = os.path.join(HERE, "_bin", "libchoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libchref.so")
 REF_BENCH = os.path.join(HERE, "_ref", "chref_bench")
 REF_MESO = os.path.join(HERE, "_ref", "meso_ref")
-REFERENCE_SRC = "/root/reference"
+REF_MESO_GPU = os.path.join(HERE, "_ref", "meso_ref_gpu")
+
+
+def reference_src() -> str | None:
+    """The reference checkout the recipe compiles: $MESO_REFERENCE, else a
+    checkout named ``reference`` beside this repository; None when neither
+    holds the reference's ``src`` tree."""
+    cands = [os.environ.get("MESO_REFERENCE", ""),
+             os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")]
+    for c in cands:
+        if c and os.path.isdir(os.path.join(c, "src", "phase_field")):
+            return os.path.abspath(c)
+    return None
 
 _i3 = ctypes.c_int * 3
 _d3 = ctypes.c_double * 3
@@ -35,13 +47,20 @@ _fp = ctypes.POINTER(ctypes.c_float)
 
 
 def build(reference: bool | None = None) -> None:
-    """Compile the C restatement, and the reference build when its sources exist."""
+    """Compile the C restatement, and the reference build when its sources
+    exist (reference_src()).  The reference driver with the GPU plugin
+    (meso_ref_gpu) is linked too when libmesogpu.so has been built."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
+    src = reference_src()
     if reference is None:
-        reference = os.path.isdir(os.path.join(REFERENCE_SRC, "src"))
+        reference = src is not None
     if reference:
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE_SRC}",
-                        f"-j{os.cpu_count() or 4}"], check=True)
+        if src is None:
+            raise FileNotFoundError("reference sources not found: set MESO_REFERENCE")
+        targets = ["ref"]
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "mesobasic_b200", "libmesogpu.so")):
+            targets.append("ref-gpu")
+        subprocess.run(["make", "-s", "-C", HERE, *targets, f"REF={src}", f"-j{os.cpu_count() or 4}"], check=True)
 
 
 def _lib(path):
@@ -206,6 +225,40 @@ def ternary_ref_run(c, n, dims, first, nsteps, Kpp=1.0, Knn=1.0, Mpp=1.0, Mnn=1.
     ref_lib().ternref_run(_i3(*dims), _d3(*spacing), dt, _i3(*bc), _ptr(prm), first, _ptr(a), _ptr(b), nsteps,
                           _ptr(oc), _ptr(on))
     return oc, on
+
+
+def ref_bench_field(dims, dt, M, kap, co, amp, gaussian, seed, nsteps, ranks, workdir, timeout=900):
+    """Runs the reference CPU build's own step loop (chref_bench: PFApp ->
+    CHBasic on SfieldFD, MPI-shim ranks as forked processes) for nsteps
+    from its seeded initial condition and returns the final field, shape
+    (nz, ny, nx), assembled from the ranks' x-slab dumps.  ranks must divide
+    nx.  Also returns the run's JSON record (wall time of the step loop)."""
+    import json
+    nx, ny, nz = dims
+    if nx % ranks:
+        raise ValueError(f"{ranks} ranks do not divide nx = {nx}")
+    prefix = os.path.join(workdir, "refdump")
+    env = dict(os.environ, MB_SHIM_NP=str(ranks), MB_SHIM_SLOT_MB=str(max(16, (ny + 2) * (nz + 2) * 8 // (1 << 20) + 2)))
+    args = [REF_BENCH, f"Domain/nx={nx}", f"Domain/ny={ny}", f"Domain/nz={nz}", f"Time/dt={dt!r}",
+            f"Time/nstep={nsteps}", f"PFApp/M={M!r}", f"PFApp/kap={kap!r}", f"PFApp/co={co!r}",
+            f"PFApp/noise_amp={amp!r}", f"PFApp/noise_type={'gaussian' if gaussian else 'uniform'}",
+            f"PFApp/seed={seed}", "PFApp/vtk=0", "PFApp/init_output=0", f"PFApp/dump_prefix={prefix}"]
+    r = subprocess.run(args, env=env, capture_output=True, text=True, timeout=timeout, cwd=workdir)
+    if r.returncode != 0:
+        raise RuntimeError(f"chref_bench failed ({r.returncode}): {r.stderr[-800:]}")
+    rec = json.loads(r.stdout.strip().splitlines()[-1])
+    out = np.empty((nz, ny, nx), dtype=np.float64)
+    for rk in range(ranks):
+        path = f"{prefix}_{nsteps}.rank{rk}"
+        with open(path, "rb") as f:
+            hdr = np.frombuffer(f.read(20), dtype=np.int32)
+            xoff, lnx, lny, lnz, step = (int(v) for v in hdr)
+            if (lny, lnz, step) != (ny, nz, nsteps):
+                raise RuntimeError(f"dump {path}: header {hdr.tolist()} does not match the run")
+            slab = np.fromfile(f, dtype=np.float64, count=lnx * lny * lnz).reshape(lnz, lny, lnx)
+        out[:, :, xoff:xoff + lnx] = slab
+        os.remove(path)
+    return out, rec
 
 
 def ref_ic(dims, co, amp, gaussian=False, seed=42) -> np.ndarray:

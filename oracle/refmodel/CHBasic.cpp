@@ -49,16 +49,18 @@ void CHBasic::generateIC(int NX, int NY, int NZ, double co, double amp, bool gau
 void CHBasic::initPhaseField()
 {
     // Seeded version of TIPSphil::initPhaseField (TIPSphil.cpp:86-103): every
-    // rank draws the global sequence and keeps its own x-slab, so the field
-    // does not depend on the rank count.
-    std::vector<double> global((size_t)p.NX * p.NY * p.NZ);
-    generateIC(p.NX, p.NY, p.NZ, co, noise_amp, noise_type == "gaussian", seed, global.data());
-    for (int i = 1; i < nx + 1; i++) {
-        for (int j = 1; j < ny + 1; j++) {
-            for (int k = 1; k < nz + 1; k++) {
-                int ndx = i * deli + j * delj + k * delk;
-                size_t ig = (size_t)(i - 1 + p.xOff);
-                c.setValue(ndx, global[ig + (size_t)p.NX * ((size_t)(j - 1) + (size_t)p.NY * (k - 1))]);
+    // rank draws the global sequence in generateIC's order (x outer) and
+    // keeps the draws of its own x-slab, so the field does not depend on the
+    // rank count.  Draws are streamed, so a rank holds only its slab (a 512^3
+    // field on 16 ranks stays at 1/16 of the grid per rank).
+    Rand rng(seed);
+    const bool gaussian = noise_type == "gaussian";
+    for (int ig = 0; ig < p.xOff + nx; ig++) {
+        const bool mine = ig >= p.xOff;
+        for (int j = 0; j < p.NY; j++) {
+            for (int k = 0; k < p.NZ; k++) {
+                double val = gaussian ? co + noise_amp * rng.normal() : co + noise_amp * (rng.uniform() - 0.5);
+                if (mine) c.setValue((ig - p.xOff + 1) * deli + (j + 1) * delj + (k + 1) * delk, val);
             }
         }
     }

@@ -112,3 +112,19 @@ def test_vtk_writer_skips_and_negative_zero(tmp_path, oracle):
     p = tmp_path / "v.vtk"
     mb.vtk_write(p, "phi", c, dims, 3, 2, 2)
     assert p.read_text() == oracle.vtk_text(c, dims, "phi", 3, 2, 2)
+
+
+def test_noalloc_rejects_tall_2d_field_on_the_host():
+    """A 2-D field (nz == 1) with more than 4096 rows is refused before any
+    device work, and the message names the ny limit (no GPU needed: the
+    pointer is never touched)."""
+    import ctypes
+    import mesobasic_b200 as mb
+    from mesobasic_b200 import _lib
+    L = _lib.load()
+    p = mb.make_params(64, 5000, 1, 0.01)
+    st = _lib.Stats()
+    rc = L.mg_field_stats_noalloc(ctypes.c_void_p(256), ctypes.byref(p), 0, None, 1000, ctypes.byref(st))
+    assert rc == _lib.MG_EINVAL
+    msg = L.mg_last_error()
+    assert b"5000 planes" in msg and b"ny of a 2-D field" in msg and b"at most 4096" in msg

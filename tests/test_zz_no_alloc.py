@@ -88,3 +88,27 @@ def test_noalloc_rejects_too_many_planes():
         assert rc == _lib.MG_OK and st["mass"] == 0.0 and st["max_abs"] == 0.0
     finally:
         L.mg_ch_destroy(h)
+
+
+def test_noalloc_counts_nonfinite_sites_like_reduce():
+    """NaN and Inf sites: both calls return MG_ENONFINITE with the same count."""
+    L = _lib.load()
+    dims = (24, 16, 8)
+    p = mb.make_params(*dims, 0.001)
+    ic = mb.ic_generate(dims, 0.0, 0.2, False, 3).reshape(-1).copy()
+    ic[[5, 77, 1000]] = np.nan
+    ic[2000] = np.inf
+    ic[2001] = -np.inf
+    h = ctypes.c_void_p()
+    _lib.check(L.mg_ch_create(ctypes.byref(p), 0, ctypes.byref(h)))
+    try:
+        _lib.check(L.mg_ch_set_field(h, ic.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        st = _lib.Stats()
+        assert L.mg_ch_reduce(h, ctypes.byref(st)) == _lib.MG_ENONFINITE
+        want = st.as_dict()
+        for _ in range(2):
+            rc, got = noalloc_stats(L, L.mg_ch_field_device(h), p, L.mg_ch_stream(h))
+            assert rc == _lib.MG_ENONFINITE, L.mg_last_error()
+            assert got["nonfinite"] == want["nonfinite"] == 5
+    finally:
+        L.mg_ch_destroy(h)
