@@ -234,9 +234,12 @@ def run_batch(mb, torch, dev, steps, sampler):
     try:
         for j, (d, c0, _, seed) in enumerate(jobs):
             b.set_field(j, mb.ic_generate(d, c0, 0.05, False, seed))
-        # warm-up (and graph capture): 4 steps, so that the mass is read
-        # after steps at which the FP32 feedback has just measured and
-        # corrected it (every 4th step)
+        # tiles chosen by the autotuner for this batch (times scratch copies,
+        # keeps the fields)
+        tuned = b.autotune(trials=5)
+        # warm-up (and graph capture): 4 steps, a multiple of the feedback
+        # cadence, so that the mass is read after steps at which the FP32
+        # feedback has just measured and corrected it
         b.step(4)
         b.sync()
         r0 = [b.reduce(j) for j in range(len(jobs))]
@@ -264,6 +267,7 @@ def run_batch(mb, torch, dev, steps, sampler):
     return {"jobs": len(jobs), "sites": sites, "steps": steps, "ms": ms,
             "value": sites * steps / (ms * 1e-3) / 1e9, "unit": "GLUPS", "precision": f"fp32 (mass feedback every {mb.MASS_EVERY} step(s))",
             "launches_per_step": info["launches_per_step"], "persistent_ctas": info["ctas"],
+            "tiles": f"autotuned: CTAs of ~{tuned['threads']} threads, z-chunks of ~{tuned['planes']} planes",
             "max_mass_drift_per_site": drift, "max_mass_drift_rel": drift_rel,
             "mass_drift_note": f"max over jobs of |M({4 + steps}) - M(4)| / sites, FP64 sums of the stored fields; the "
                                f"feedback measures and corrects the mass after every {mb.MASS_EVERY} step(s)",
@@ -544,7 +548,7 @@ def run_ours(args, rank, world, local_rank):
                  "mass_correct": mb.MASS_EVERY},
         "batch": None if not batch else {
             "value": batch["value"], "roofline_frac": batch["roofline_frac"], "jobs": batch["jobs"],
-            "steps": batch["steps"], "launches_per_step": batch["launches_per_step"],
+            "steps": batch["steps"], "launches_per_step": batch["launches_per_step"], "tiles": batch["tiles"],
             "max_mass_drift_per_site": batch["max_mass_drift_per_site"],
             "max_mass_drift_rel": batch["max_mass_drift_rel"]},
         "serve": None if not serve else {

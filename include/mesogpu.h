@@ -55,9 +55,11 @@ typedef struct {
                               errors of the field do not accumulate as a
                               drift of total mass.  The stored mass is on
                               target (to half a nudge) after every K-th step.
-                              K = 1 measures every step; the Python mirror
-                              and the driver default to K = 4, at a quarter
-                              of the measuring cost */
+                              K = 1 measures every step and holds the
+                              relative drift within 1e-10 at every step; the
+                              Python mirror and the driver default to K = 1.
+                              K = 4 costs a quarter of the measuring and is
+                              on target at every 4th step only */
     double noise;          /* >0: after each step every site gets
                               c += dt * (noise * (u - 0.5)), u uniform in (0,1)
                               [PFApp/noiseStr] (TIPSphil.cpp:200-209); 0: off */
@@ -284,6 +286,16 @@ int mg_batch_write_vtk(mg_batch_t* b, int job, const char* path, const char* tag
 void* mg_batch_stream(mg_batch_t* b);
 /* Items (tiles) and persistent CTAs of the batch's launches. */
 int mg_batch_info(const mg_batch_t* b, int* nitems, int* nctas, int* nlaunch_per_step);
+/* Chooses the batch's tiles by measurement: every job is tiled for CTAs of
+ * about `threads` threads and z-chunks of about `planes` planes (the same
+ * targets for all jobs, so the CTAs of the shared launch are equally full);
+ * each candidate pair is timed over `trials` steps of a scratch copy of the
+ * batch (same shapes and parameters, zero fields, so the batch's own fields
+ * and step counts are untouched).  The best pair re-tiles the batch (results
+ * do not depend on the tiling) and is stored in the tuning cache under the
+ * batch's composition, where mg_batch_create finds it for later batches of
+ * the same mix.  No reference counterpart. */
+int mg_batch_autotune(mg_batch_t* b, int trials, int* threads, int* planes, double* ms_per_step);
 void mg_batch_destroy(mg_batch_t* b);
 
 /* ----------------------------------------------------------------------

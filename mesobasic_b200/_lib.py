@@ -130,6 +130,7 @@ SIGNATURES = {
     "mg_batch_stream": (_vp, [_vp]),
     "mg_batch_info": (ctypes.c_int, [_vp, _P(ctypes.c_int), _P(ctypes.c_int), _P(ctypes.c_int)]),
     "mg_batch_destroy": (None, [_vp]),
+    "mg_batch_autotune": (ctypes.c_int, [_vp, ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_int), _P(ctypes.c_double)]),
     "mg_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _P(_vp)]),
     "mg_server_submit": (ctypes.c_int, [_vp, _P(Params), _dp, ctypes.c_longlong, _P(ctypes.c_longlong)]),
     "mg_server_poll": (ctypes.c_int, [_vp, ctypes.c_longlong, _P(ctypes.c_int)]),

@@ -28,9 +28,9 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["engine.cu", "capi.cu", "server.cu", "noalloc.cu", "vtk_device.cu"]
+CU_SOURCES = ["engine.cu", "march_f32.cu", "march_f64.cu", "capi.cu", "server.cu", "noalloc.cu", "vtk_device.cu"]
 CPP_SOURCES = ["host_io.cpp"]
-HEADERS = ["ch_kernels.cuh", "ch_lean.cuh", "ch_types.h", "mg_device.cuh", "engine.h"]
+HEADERS = ["ch_device.cuh", "ch_kernels.cuh", "ch_lean.cuh", "ch_march.cuh", "ch_types.h", "mg_device.cuh", "engine.h"]
 DRIVER_SOURCES = ["input_file.cpp", "pf_model.cpp", "chbasic_gpu.cpp", "tipsphil_gpu.cpp", "sips_gpu.cpp", "meso_b200.cpp"]
 
 
@@ -55,6 +55,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "mesogpu.h")]
     objs = []
+    jobs = []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
@@ -62,9 +63,19 @@ def build(verbose: bool = False, force: bool = False) -> str:
         if force or _newer(o, [s] + headers):
             flags = [NVCC, *ARCH, "-Xptxas=-v", "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
                      f"-I{INCLUDE}", f"-I{CSRC}", "-c", s, "-o", o]
-            out = _run(flags, verbose)
-            with open(os.path.join(BUILD, src + ".ptxas.txt"), "w") as f:  # registers / spills per kernel
-                f.write(out)
+            jobs.append((src, flags))
+
+    def compile_one(job):
+        src, flags = job
+        out = _run(flags, verbose)
+        with open(os.path.join(BUILD, src + ".ptxas.txt"), "w") as f:  # registers / spills per kernel
+            f.write(out)
+        return out
+
+    # the translation units compile independently: run them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for out in ex.map(compile_one, jobs):
             if verbose and out:
                 print(out)
     for src in CPP_SOURCES:

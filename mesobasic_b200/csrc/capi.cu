@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <string>
 #include <climits>
 #include <cmath>
 #include <cstdlib>
@@ -21,6 +23,7 @@ struct mg_ch {
 struct mg_batch {
     mg::Engine eng;
     std::vector<mg::Job*> jobs;
+    std::vector<mg_ch_params> params;  // as created (mg_batch_autotune builds scratch copies)
 };
 
 using mg::fail;
@@ -336,6 +339,24 @@ int mg_autotune(const mg_ch_params* params, int device, int trials, mg_tiling* b
 }
 
 // ---------------------------------------------------------------- batch
+// The composition of a batch (job shapes, precision and mass feedback, with
+// their counts): the tuning-cache key of its tiles.
+static std::string batch_signature(const mg_ch_params* jobs, int njobs)
+{
+    std::map<std::string, int> count;
+    for (int i = 0; i < njobs; ++i) {
+        mg::Geometry g;
+        if (mg::make_geometry(jobs[i], &g) != MG_OK) {
+            mg::clear_error();
+            continue;
+        }
+        count[mg::tune_key(g) + (jobs[i].mass_correct ? ":m" : "")] += 1;
+    }
+    std::string s = "batch";
+    for (auto& kv : count) s += "|" + kv.first + "*" + std::to_string(kv.second);
+    return s;
+}
+
 int mg_batch_create(const mg_ch_params* jobs, int njobs, int device, mg_batch_t** out)
 {
     mg::clear_error();
@@ -349,8 +370,18 @@ int mg_batch_create(const mg_ch_params* jobs, int njobs, int device, mg_batch_t*
     if (!b) return fail(MG_ENOMEM, "host allocation failed");
     MG_TRY(b->eng.init(device, njobs));
     b->eng.batch_tiling = true;
-    b->eng.batch_threads = mg::mg_env_int("MG_BATCH_THREADS", 320);
-    b->eng.batch_planes = mg::mg_env_int("MG_BATCH_PLANES", 128);
+    // tile targets: the environment, else what mg_batch_autotune measured for
+    // this composition, else 320 threads and 128-plane chunks
+    b->eng.batch_threads = 320;
+    b->eng.batch_planes = 128;
+    b->params.assign(jobs, jobs + njobs);
+    mg_tiling tuned;
+    if (mg::tune_lookup(batch_signature(jobs, njobs), &tuned)) {
+        b->eng.batch_threads = tuned.ty;
+        b->eng.batch_planes = tuned.nchunk;
+    }
+    b->eng.batch_threads = mg::mg_env_int("MG_BATCH_THREADS", b->eng.batch_threads);
+    b->eng.batch_planes = mg::mg_env_int("MG_BATCH_PLANES", b->eng.batch_planes);
     for (int i = 0; i < njobs; ++i) {
         mg::Job* j = nullptr;
         int rc = b->eng.add_job(jobs[i], -1, &j);
@@ -424,6 +455,91 @@ int mg_batch_info(const mg_batch_t* b, int* nitems, int* nctas, int* nlaunch)
     if (nitems) *nitems = b->eng.nitems_total();
     if (nctas) *nctas = b->eng.nctas_total();
     if (nlaunch) *nlaunch = b->eng.nlaunch_per_step();
+    return MG_OK;
+}
+
+// ms per step of a scratch batch with these tile targets (zero fields)
+static int time_batch_targets(const std::vector<mg_ch_params>& params, int device, int threads, int planes,
+                              int trials, double* ms, std::vector<mg_tiling>* tilings)
+{
+    mg::Engine e;
+    MG_TRY(e.init(device, (int)params.size()));
+    e.batch_tiling = true;
+    e.batch_threads = threads;
+    e.batch_planes = planes;
+    tilings->clear();
+    for (const mg_ch_params& p : params) {
+        mg::Job* j = nullptr;
+        MG_TRY(e.add_job(p, -1, &j));
+        MG_CUDA(cudaMemsetAsync(j->buf[0], 0, j->g.n * j->g.es, e.stream));
+        MG_CUDA(cudaMemsetAsync(j->buf[1], 0, j->g.n * j->g.es, e.stream));
+        tilings->push_back(j->tiling);
+    }
+    MG_TRY(e.enqueue_steps(2));  // warm-up (also captures the graph)
+    cudaEvent_t e0, e1;
+    MG_CUDA(cudaEventCreate(&e0));
+    MG_CUDA(cudaEventCreate(&e1));
+    cudaEventRecord(e0, e.stream);
+    int rc = e.enqueue_steps(trials);
+    cudaEventRecord(e1, e.stream);
+    cudaEventSynchronize(e1);
+    float f = 0.f;
+    cudaEventElapsedTime(&f, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    MG_TRY(rc);
+    MG_TRY(e.sync(-1));
+    *ms = f / trials;
+    return MG_OK;
+}
+
+int mg_batch_autotune(mg_batch_t* b, int trials, int* threads, int* planes, double* ms_per_step)
+{
+    mg::clear_error();
+    if (!b) return fail(MG_EINVAL, "null handle");
+    if (trials < 1) trials = 5;
+    MG_TRY(b->eng.sync(-1));
+    double best = 1e30;
+    int bt = b->eng.batch_threads, bp = b->eng.batch_planes;
+    std::vector<mg::Geometry> geo(b->params.size());
+    for (size_t i = 0; i < geo.size(); ++i) MG_TRY(mg::make_geometry(b->params[i], &geo[i]));
+    std::vector<std::vector<int>> seen;  // candidates that tile every job alike are timed once
+    for (int t : {192, 256, 320, 384, 448, 512, 640})
+        for (int p : {32, 64, 128, 256}) {
+            std::vector<int> sig;
+            for (const mg::Geometry& g : geo) {
+                const mg_tiling tt = mg::batch_tiling_for(g, b->eng.info, b->eng.device, t, p);
+                sig.insert(sig.end(), {tt.ty, tt.nchunk, tt.nbuf, tt.path});
+            }
+            if (std::find(seen.begin(), seen.end(), sig) != seen.end()) continue;
+            seen.push_back(sig);
+            double ms;
+            std::vector<mg_tiling> tl;
+            if (time_batch_targets(b->params, b->eng.device, t, p, trials, &ms, &tl) != MG_OK) {
+                mg::clear_error();
+                cudaGetLastError();
+                continue;
+            }
+            if (ms < best) {
+                best = ms;
+                bt = t;
+                bp = p;
+            }
+        }
+    if (best >= 1e30) return fail(MG_ECUDA, "no tile target could be timed");
+    // re-tile the batch (the fields and step counts stay)
+    b->eng.batch_threads = bt;
+    b->eng.batch_planes = bp;
+    for (mg::Job* j : b->jobs) {
+        const mg_tiling t = mg::batch_tiling_for(j->g, b->eng.info, b->eng.device, bt, bp);
+        if (t.ty != j->tiling.ty || t.nchunk != j->tiling.nchunk || t.nbuf != j->tiling.nbuf || t.path != j->tiling.path)
+            MG_TRY(b->eng.set_tiling(j, t));
+    }
+    mg::tune_store(batch_signature(b->params.data(), (int)b->params.size()), mg_tiling{bt, bp, mg::kMarchBatchNbuf, 0},
+                   best);
+    if (threads) *threads = bt;
+    if (planes) *planes = bp;
+    if (ms_per_step) *ms_per_step = best;
     return MG_OK;
 }
 

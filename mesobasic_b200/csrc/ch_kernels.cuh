@@ -31,334 +31,9 @@
 // substituting the centre value for an out-of-domain neighbour.
 #pragma once
 
-#include "ch_types.h"
-#include "mg_device.cuh"
+#include "ch_device.cuh"
 
 namespace mg {
-
-// ---------------------------------------------------------------- strips
-// A thread owns a 32-byte strip of one row: 8 floats or 4 doubles.  FP32
-// strips are held as four 64-bit pairs so the arithmetic can use the paired
-// f32x2 instructions of sm_100.
-
-template <typename T>
-struct Strip;
-
-template <>
-struct Strip<float> {
-    static constexpr int W = 8;
-    unsigned long long p[4];
-    __device__ __forceinline__ float get(int e) const
-    {
-        float a, b;
-        asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(p[e >> 1]));
-        return (e & 1) ? b : a;
-    }
-};
-
-template <>
-struct Strip<double> {
-    static constexpr int W = 4;
-    double v[4];
-    __device__ __forceinline__ double get(int e) const { return v[e]; }
-};
-
-__device__ __forceinline__ unsigned long long pk2(float a, float b)
-{
-    unsigned long long r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-    return r;
-}
-__device__ __forceinline__ float2 upk2(unsigned long long r)
-{
-    float2 a;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
-    return a;
-}
-__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b)
-{
-    unsigned long long r;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b)
-{
-    unsigned long long r;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b)
-{
-    unsigned long long r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c)
-{
-    unsigned long long r;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
-    return r;
-}
-__device__ __forceinline__ unsigned long long splat2(float a) { return pk2(a, a); }
-
-// A strip is two 16-byte halves: half A at p, half B at p + off (the
-// halves of neighbouring threads are adjacent, so every warp-wide access is
-// one contiguous run and free of bank conflicts).
-template <typename T>
-__device__ __forceinline__ Strip<T> ld_strip(const T* p, int off)
-{
-    Strip<T> s;
-    if constexpr (sizeof(T) == 4) {
-        const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(p);
-        const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(p + off);
-        s.p[0] = a.x, s.p[1] = a.y, s.p[2] = b.x, s.p[3] = b.y;
-    } else {
-        const double2 a = *reinterpret_cast<const double2*>(p);
-        const double2 b = *reinterpret_cast<const double2*>(p + off);
-        s.v[0] = a.x, s.v[1] = a.y, s.v[2] = b.x, s.v[3] = b.y;
-    }
-    return s;
-}
-
-template <typename T>
-__device__ __forceinline__ void st_strip(T* p, int off, const Strip<T>& s)
-{
-    if constexpr (sizeof(T) == 4) {
-        *reinterpret_cast<ulonglong2*>(p) = make_ulonglong2(s.p[0], s.p[1]);
-        *reinterpret_cast<ulonglong2*>(p + off) = make_ulonglong2(s.p[2], s.p[3]);
-    } else {
-        *reinterpret_cast<double2*>(p) = make_double2(s.v[0], s.v[1]);
-        *reinterpret_cast<double2*>(p + off) = make_double2(s.v[2], s.v[3]);
-    }
-}
-
-template <typename T>
-__device__ __forceinline__ void zero_strip(Strip<T>& s)
-{
-    if constexpr (sizeof(T) == 4) {
-        s.p[0] = s.p[1] = s.p[2] = s.p[3] = 0ull;
-    } else {
-        s.v[0] = s.v[1] = s.v[2] = s.v[3] = 0.0;
-    }
-}
-
-// Laplacian numerator sums of a strip with paired FP32 arithmetic, SIMPLE
-// geometry (all periodic, equal spacing): per pair
-// (x sum) + (y sum) + (z sum) - 2*dims*centre.  Half A is pairs 0-1 with x
-// neighbours lA/rA, half B pairs 2-3 with lB/rB.
-template <bool FLAT>
-__device__ __forceinline__ void lap_pairs(const Strip<float>& c, float lA, float rA, float lB, float rB,
-                                          const Strip<float>& up, const Strip<float>& dn, const Strip<float>& zlo,
-                                          const Strip<float>& zhi, unsigned long long (&out)[4])
-{
-    const unsigned long long m6 = splat2(FLAT ? -4.f : -6.f);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int h = k >> 1;  // half
-        const float xm0 = (k & 1) == 0 ? (h == 0 ? lA : lB) : c.get(2 * k - 1);
-        const float xp1 = (k & 1) == 1 ? (h == 0 ? rA : rB) : c.get(2 * k + 2);
-        const unsigned long long sx = pk2(xm0 + c.get(2 * k + 1), c.get(2 * k) + xp1);
-        unsigned long long sacc = add2(sx, add2(zlo.p[k], zhi.p[k]));
-        if constexpr (!FLAT) sacc = add2(sacc, add2(up.p[k], dn.p[k]));
-        out[k] = fma2(c.p[k], m6, sacc);
-    }
-}
-
-// (a[+] + a[-] - 2*a) scaled by c: multiply (power-of-two spacing, exact) or
-// divide (otherwise), as SfieldFD::Laplacian writes it (SfieldFD.cpp:296-302).
-template <typename T>
-__device__ __forceinline__ T axis_term(T plus, T minus, T centre, double c, bool divide)
-{
-    using A = Arith<T>;
-    T num = A::sub(A::add(plus, minus), A::mul(T(2), centre));
-    return divide ? A::div(num, T(c)) : A::mul(num, T(c));
-}
-
-// The 7-point Laplacian of one site in the reference's order
-// ((lapx + lapy) + lapz), SfieldFD.cpp:296-302.  FLAT drops the y term,
-// which is exactly zero in the reference for a flat axis.  SIMPLE (every
-// axis periodic, equal spacing): FP64 skips the multiplications by
-// 1/d^2 = 1, which are exact identities; FP32 uses the algebraically equal
-// ((sum of six neighbours) - 6c) / d^2.
-template <typename T, bool FLAT, bool SIMPLE>
-__device__ __forceinline__ T lap7(T c0, T xp, T xm, T yp, T ym, T zp, T zm, double cx, double cy, double cz,
-                                  bool divX, bool divY, bool divZ)
-{
-    using A = Arith<T>;
-    if constexpr (SIMPLE) {
-        if constexpr (sizeof(T) == 8) {
-            const T c2 = A::mul(T(2), c0);
-            const T lx = A::sub(A::add(xp, xm), c2);
-            const T lz = A::sub(A::add(zp, zm), c2);
-            if constexpr (FLAT) {
-                return A::add(lx, lz);
-            } else {
-                const T ly = A::sub(A::add(yp, ym), c2);
-                return A::add(A::add(lx, ly), lz);
-            }
-        } else {
-            T s = (xp + xm) + (zp + zm);
-            if constexpr (!FLAT) s += (yp + ym);
-            return fmaf(FLAT ? -4.f : -6.f, c0, s) * (float)cx;
-        }
-    } else {
-        if constexpr (FLAT) {
-            return A::add(axis_term(xp, xm, c0, cx, divX), axis_term(zp, zm, c0, cz, divZ));
-        } else {
-            return A::add(A::add(axis_term(xp, xm, c0, cx, divX), axis_term(yp, ym, c0, cy, divY)),
-                          axis_term(zp, zm, c0, cz, divZ));
-        }
-    }
-}
-
-// mu = (c*c*c - c) - kappa*lap (FP64 in that order; FP32 contracted)
-template <typename T>
-__device__ __forceinline__ T chem_pot(T c0, T lap, T kap)
-{
-    if constexpr (sizeof(T) == 8) {
-        using A = Arith<T>;
-        return A::sub(A::sub(A::mul(A::mul(c0, c0), c0), c0), A::mul(kap, lap));
-    } else {
-        return fmaf(-kap, lap, fmaf(c0 * c0, c0, -c0));
-    }
-}
-
-// MurmurHash3's 32-bit finaliser (public domain): a bijective mixer.
-__device__ __forceinline__ uint32_t fmix32(uint32_t h)
-{
-    h ^= h >> 16;
-    h *= 0x85ebca6bu;
-    h ^= h >> 13;
-    h *= 0xc2b2ae35u;
-    h ^= h >> 16;
-    return h;
-}
-
-__device__ __forceinline__ int wrap_or_clamp(int i, int n, bool periodic)
-{
-    if (periodic) {
-        i %= n;
-        return i < 0 ? i + n : i;
-    }
-    return i < 0 ? 0 : (i >= n ? n - 1 : i);
-}
-
-// Locate job for a flat item index (item_begin is ascending).
-__device__ __forceinline__ int find_job(const int* item_begin, int njobs, int item)
-{
-    int lo = 0, hi = njobs - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (__ldg(item_begin + mid) <= item) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
-// The stored mass of one thread strip in 2^-32 units: its 8 values summed
-// in FP64 (exact conversions, fixed order), rounded once.  The same function
-// measures the field at upload and after every measured step.
-__device__ __forceinline__ long long strip_mass(float o0, float o1, float o2, float o3, float o4, float o5, float o6,
-                                                float o7)
-{
-    const double x = ((double)o0 + (double)o2) + ((double)o4 + (double)o6);
-    const double y = ((double)o1 + (double)o3) + ((double)o5 + (double)o7);
-    return __double2ll_rn((x + y) * (double)kMassScale);
-}
-
-// Does the nudge window [w0, w0 + |cnt|) (wrapping at nsites) reach the row
-// of sites [rs, rs + len)?  Asked only in planes the window reaches, so that
-// only the threads of the rows it covers take the out-of-line nudge.
-__device__ __forceinline__ bool window_reaches(long long rs, long long len, long long w0, long long cnt,
-                                               long long nsites)
-{
-    const long long w1 = w0 + (cnt < 0 ? -cnt : cnt);
-    if (rs < w1 && rs + len > w0) return true;
-    return w1 > nsites && rs < w1 - nsites;
-}
-
-// Adds the mass nudge to the elements of a thread's 8-float strip whose sites
-// lie in the nudge window (sites of element e: site0 + e for e < 4, site0 +
-// offB + e - 4 for the second half).  Called only for planes the window
-// reaches, so it stays out of line.
-__device__ __noinline__ void nudge_strip(float* o, long long site0, long long offB, long long w0, long long cnt,
-                                         long long nsites)
-{
-    const long long na = cnt < 0 ? -cnt : cnt;
-    const float nudge = cnt < 0 ? -kNudge : kNudge;
-    for (int e = 0; e < 8; ++e) {
-        long long r = site0 + (e < 4 ? e : offB + e - 4) - w0;
-        if (r < 0) r += nsites;
-        if (r < na) o[e] += nudge;
-    }
-}
-
-// FP32 mass feedback at the end of a step, run by the whole CTA that
-// finished the job's last item of the step (every item has stored its part
-// of the new field and fenced it).  The nudges this step added inside the
-// stencil are booked.  On a measured step the stored mass M (the items'
-// partial sums in item order) gives:
-//  - the correction: round((target - M) / kNudge) nudges, added here to
-//    consecutive sites of the new field, so the stored mass leaves every
-//    measured step on target;
-//  - the rounding defect of the interval since the last measure (the change
-//    of stored mass the nudges did not make), d per step: each step of the
-//    coming interval adds round(-d / kNudge) nudges inside the stencil, so
-//    the mass stays on target between measures while rounding losses are
-//    systematic (they are while the field evolves slowly).
-// kNudge is a multiple of the unit in the last place of every float below 2
-// in magnitude, so each nudge moves the stored sum by exactly its size.  The
-// window of nudged sites moves on by a golden-ratio fraction of the field
-// every step.
-__device__ __forceinline__ void mass_feedback_step_end(JobDev* J, bool measure, long long nsites, int nitems_job,
-                                                       float* field, SmemHead* head)
-{
-    const int tid = threadIdx.x, lane = tid & 31;
-    const long long stride = (long long)(0.6180339887498949 * (double)nsites) | 1;
-    if (tid < 32) {
-        __int128 r = 0;
-        if (measure) {
-            for (int k = lane; k < nitems_job; k += 32) r += __ldcg(J->partial + k);
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const unsigned long long lo = __shfl_down_sync(0xffffffffu, (unsigned long long)r, off);
-                const long long hi = __shfl_down_sync(0xffffffffu, (long long)(r >> 64), off);
-                r += ((__int128)hi << 64) | (__int128)lo;
-            }
-        }
-        if (lane == 0) {
-            J->nudge_applied += J->nudge_count;
-            long long now = 0;
-            if (measure) {
-                const double mm = (double)r / (double)kMassScale;
-                const double d =
-                    ((mm - J->mass_last) - (double)J->nudge_applied * (double)kNudge) / (double)J->mass_every;
-                double k = rint((J->mass_target - mm) / (double)kNudge);
-                double kr = rint(-d / (double)kNudge);
-                k = fmin(fmax(k, -(double)nsites), (double)nsites);
-                kr = fmin(fmax(kr, -(double)nsites), (double)nsites);
-                now = (long long)k;
-                J->mass_last = mm + k * (double)kNudge;
-                J->nudge_applied = 0;
-                J->nudge_rest = (long long)kr;
-            }
-            head->nudge_begin = J->nudge_begin;
-            head->nudge_count = now;
-            const long long w = now != 0 ? (J->nudge_begin + stride) % nsites : J->nudge_begin;
-            J->nudge_count = J->nudge_rest;
-            J->nudge_begin = (w + stride) % nsites;
-        }
-    }
-    __syncthreads();
-    const long long cnt = head->nudge_count, w0 = head->nudge_begin;
-    const long long na = cnt < 0 ? -cnt : cnt;
-    const float nudge = cnt < 0 ? -kNudge : kNudge;
-    for (long long q = tid; q < na; q += blockDim.x) {
-        long long site = w0 + q;
-        if (site >= nsites) site -= nsites;
-        field[site] = __ldcg(field + site) + nudge;
-    }
-}
 
 // NXC: row width fixed at compile time (0: read from the job), so that row,
 // half and piece offsets fold into instruction immediates.
@@ -880,21 +555,6 @@ __global__ void ch_step_generic_kernel(JobDev* job)
 // job's seed, with counter (site / 4, step): four sites per draw, r =
 // (word + 0.5) * 2^-32, so r depends on (seed, site, step) only.
 
-__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
-{
-#pragma unroll
-    for (int r = 0; r < 10; ++r) {
-        if (r) {
-            k.x += 0x9E3779B9u;
-            k.y += 0xBB67AE85u;
-        }
-        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
-        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
-        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
-    }
-    return c;
-}
-
 // Adds the noise of the step just taken (the job's step counter) once: a
 // replayed graph step that skipped the job leaves noise_step == step, and
 // the blocks return.  The last block to finish records the step.
@@ -966,40 +626,6 @@ __device__ __forceinline__ size_t fh_at(int x, int y, int z, const JobDev& J)
     return ((size_t)z * J.ny + y) * J.nx + x;
 }
 
-// SIPS: mu and mobility of one site (SIPS.cpp:160-208 with getFHcc,
-// philliesDiffusion and secondDerFH of SIPS.cpp:254-285)
-__device__ __forceinline__ void sips_site(const FhDev& F, double cc, double lapc, double kap, int x, double step,
-                                          double dt, double* mu, double* mob)
-{
-    using A = Arith<double>;
-    const double kT = A::div(F.Tinit, 273.0);
-    double chi;
-    if (x >= F.NSdepth)
-        chi = A::add(A::mul(A::sub(F.chiPS, F.chiPN),
-                            erf(A::div((double)(x + 1), A::mul(2.0, sqrt(A::mul(A::mul(F.chiCond, step), dt)))))),
-                     F.chiPN);
-    else
-        chi = F.chiPN;
-    const double cfh = cc < 0.0 ? 0.001 : (cc > 1.0 ? 0.999 : cc);
-    double df = A::add(A::sub(A::sub(A::div(A::add(log(cfh), 1.0), F.N), log(A::sub(1.0, cfh))), 1.0),
-                       A::mul(chi, A::sub(1.0, A::mul(2.0, cfh))));
-    if (cc <= 0.0) df = A::mul(A::mul(-1.5, F.A), sqrt(-cc));
-    *mu = A::sub(df, A::mul(kap, lapc));
-    double cphil;
-    if (cc >= 1.0) cphil = A::div(A::mul(1.0, F.Mweight), F.Mvolume);
-    else if (cc < 0.0) cphil = A::div(A::mul(0.000001, F.Mweight), F.Mvolume);
-    else cphil = A::div(A::mul(cc, F.Mweight), F.Mvolume);
-    double ddf = A::mul(0.5, A::add(A::div(1.0, A::mul(F.N, cc)), A::div(1.0, A::sub(1.0, cc))));
-    ddf = A::mul(ddf, kT);
-    const double Dp = A::mul(F.D0, exp(A::mul(-F.gamma, pow(cphil, F.nu))));
-    double Mc = A::div(Dp, ddf);
-    const double frac = A::div(A::sub(chi, F.chiPS), A::sub(F.chiPN, F.chiPS));
-    const double scale = A::add(0.95, A::mul(0.25, log(A::sub(1.0225, frac))));
-    if (Mc > 1.0) Mc = 1.0;
-    else if (Mc < 0.00001) Mc = 0.00001;
-    *mob = A::mul(Mc, scale);
-}
-
 __global__ void fh_mu_mob_kernel(JobDev* job)
 {
     using A = Arith<double>;
@@ -1025,54 +651,7 @@ __global__ void fh_mu_mob_kernel(JobDev* job)
         lapc = A::add(A::add(axis_term(xp, xm, cc, J.cx, J.flags & JF_DIV_X), axis_term(yp, ym, cc, J.cy, J.flags & JF_DIV_Y)),
                       axis_term(zp, zm, cc, J.cz, J.flags & JF_DIV_Z));
     }
-    if (F.model == kFhLinear) {
-        F.mu[s] = A::sub(0.0, A::mul(J.kap, lapc));
-        F.mob[s] = F.Mconst;
-        return;
-    }
-    if (F.model == kFhSips) {
-        sips_site(F, cc, lapc, J.kap, x, cs, J.dtM_dt, F.mu + s, F.mob + s);
-        return;
-    }
-    // temperature of the step: a uniform ramp, or the bath profile along x
-    // (TIPSbathPHIL.cpp:118-121)
-    double T;
-    if (F.model == kFhBath)
-        T = A::add(A::mul(A::sub(F.Tinit, F.Tbath),
-                          erf(A::div((double)(x + 1), A::mul(2.0, sqrt(A::mul(A::mul(F.thermCond, cs), J.dtM_dt)))))),
-                   F.Tbath);
-    else
-        T = A::sub(F.Tinit, A::mul(A::sub(F.Tinit, F.Tbath), A::div(cs, (double)F.nstep)));
-    const double kT = A::div(T, 273.0);
-    const double chi = A::add(A::div(F.alpha, T), F.beta);
-    // chemical potential: df = ((log(cc)+1)/N - log(1-cc) - 1 + chi*(1-2cc)) * kT
-    double df = A::add(A::sub(A::sub(A::div(A::add(log(cc), 1.0), F.N), log(A::sub(1.0, cc))), 1.0),
-                       A::mul(chi, A::sub(1.0, A::mul(2.0, cc))));
-    df = A::mul(df, kT);
-    if (cc <= 0.0) df = A::mul(A::mul(-1.5, F.A), sqrt(-cc));
-    F.mu[s] = A::sub(df, A::mul(J.kap, lapc));
-    // Phillies self-diffusion over the second derivative of the free energy
-    double cc_phil, ddf;
-    if (cc >= 1.0) {
-        cc_phil = A::div(A::mul(1.0, F.Mweight), F.Mvolume);
-        ddf = A::mul(0.5, A::add(A::div(1.0, A::mul(F.N, 0.999)), A::div(1.0, A::sub(1.0, 0.999))));
-    } else if (cc < 0.0) {
-        const double cm = 0.0001;
-        cc_phil = A::div(A::mul(cm, F.Mweight), F.Mvolume);
-        ddf = A::mul(0.5, A::add(A::div(1.0, A::mul(F.N, cm)), A::div(1.0, A::sub(1.0, cm))));
-    } else {
-        cc_phil = A::div(A::mul(cc, F.Mweight), F.Mvolume);
-        ddf = A::mul(0.5, A::add(A::div(1.0, A::mul(F.N, cc)), A::div(1.0, A::sub(1.0, cc))));
-    }
-    ddf = A::mul(ddf, kT);
-    double D = A::mul(F.D0, A::div(T, F.Tinit));
-    if (D > F.D0) D = F.D0;
-    const double Dp = A::mul(D, exp(A::mul(-F.gamma, pow(cc_phil, F.nu))));
-    double Mc = A::div(Dp, ddf);
-    if (Mc < 0.000001) Mc = 0.000001;
-    if (Mc > F.D0) Mc = F.D0;
-    if (T <= F.Tcrystal) Mc = A::mul(Mc, 0.001);
-    F.mob[s] = Mc;
+    fh_site(F, cc, lapc, J.kap, x, cs, J.dtM_dt, F.mu + s, F.mob + s);
 }
 
 // (a[-]*b1 + a[+]*b2 - (b1+b2)*a) / d^2 with b1, b2 the harmonic means of

@@ -17,35 +17,6 @@
 
 namespace mg {
 
-__device__ __forceinline__ void lds_v2(uint32_t addr, unsigned long long& x, unsigned long long& y)
-{
-    asm volatile("ld.shared.v2.u64 {%0, %1}, [%2];" : "=l"(x), "=l"(y) : "r"(addr) : "memory");
-}
-__device__ __forceinline__ void sts_v2(uint32_t addr, unsigned long long x, unsigned long long y)
-{
-    asm volatile("st.shared.v2.u64 [%0], {%1, %2};" ::"r"(addr), "l"(x), "l"(y) : "memory");
-}
-__device__ __forceinline__ void stg_v2(void* p, unsigned long long x, unsigned long long y)
-{
-    asm volatile("st.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(x), "l"(y) : "memory");
-}
-// strip of 8 floats: half A at addr, half B at addr + offB
-__device__ __forceinline__ Strip<float> lds_strip(uint32_t addr, uint32_t offB)
-{
-    Strip<float> s;
-    lds_v2(addr, s.p[0], s.p[1]);
-    lds_v2(addr + offB, s.p[2], s.p[3]);
-    return s;
-}
-__device__ __forceinline__ void tma_load_3d_s(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y, int z)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "r"(z)
-        : "memory");
-}
-
 template <int NXC, int NBUF, bool MASS>
 __global__ void __launch_bounds__(kMaxBlock, 1) ch_lean_kernel(StepArgs a)
 {

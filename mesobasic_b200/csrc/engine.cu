@@ -3,6 +3,8 @@
 #include "engine.h"
 #include "ch_kernels.cuh"
 #include "ch_lean.cuh"
+#include "ch_march.cuh"
+#include "fh_march.cuh"
 
 #include <cufft.h>
 #include <dlfcn.h>
@@ -227,6 +229,80 @@ int plan_tiling(const Geometry& g, const mg_tiling& t, const DevInfo& d, TilePla
     return MG_OK;
 }
 
+// The fused variable-mobility kernel (fh_march.cuh) takes FP64 rows of at
+// most 256 elements whose width is a multiple of 16 (128-byte aligned
+// shared-memory rows for the TMA), 3-D with ny >= 2 or flat.
+bool fh_shape_ok(const Geometry& g)
+{
+    return g.es == 8 && g.lnx % 16 == 0 && g.lnx <= kFhMaxNx && (g.flat || g.lny >= 2);
+}
+
+static size_t fh_smem(int nbuf, int cplane, int mplane)
+{
+    const size_t head = (sizeof(SmemHead) + 127) / 128 * 128 + 128;  // + alignment slack
+    return head + (size_t)nbuf * cplane * 8 + (size_t)6 * mplane * 8 + (size_t)kFhMaxNx * sizeof(FhCol);
+}
+
+int plan_fh_tiling(const Geometry& g, const mg_tiling& t, const DevInfo& d, TilePlan* out)
+{
+    TilePlan pl;
+    if (t.path == 1) {
+        pl.tma_ok = false;
+        pl.block = 256;
+        pl.nitems = 1;
+        *out = pl;
+        return MG_OK;
+    }
+    if (t.path != 0) return fail(MG_EINVAL, "tiling path must be 0 or 1");
+    if (!fh_shape_ok(g)) return fail(MG_EINVAL, "shape %dx%dx%d is not taken by the fused variable-mobility kernel",
+                                     g.lnx, g.lny, g.lnz);
+    if (t.nbuf != 3) return fail(MG_EINVAL, "the fused variable-mobility kernel uses nbuf 3");
+    if (t.nchunk < 1 || t.nchunk > g.lnz) return fail(MG_EINVAL, "nchunk %d outside [1, %d]", t.nchunk, g.lnz);
+    int CY = 1, MY = 1;
+    if (g.flat) {
+        if (t.ty != 1) return fail(MG_EINVAL, "2-D jobs use ty = 1");
+        pl.ntile = 1;
+    } else {
+        if (t.ty < 1 || t.ty > g.lny) return fail(MG_EINVAL, "ty %d must be in [1, ny] (ny = %d)", t.ty, g.lny);
+        CY = t.ty + 4;
+        MY = t.ty + 2;
+        pl.ntile = (g.lny + t.ty - 1) / t.ty;
+    }
+    if ((g.lnx / 4) * MY > kFhBlock) return fail(MG_EINVAL, "tile needs %d threads (> %d); lower ty", (g.lnx / 4) * MY, kFhBlock);
+    pl.block = kFhBlock;
+    pl.cplane = round_up(CY * g.lnx, 32);
+    pl.mplane = round_up(MY * g.lnx, 32);
+    pl.smem = fh_smem(t.nbuf, pl.cplane, pl.mplane);
+    if (pl.smem > d.smem_optin)
+        return fail(MG_EINVAL, "tile needs %zu bytes of shared memory (> %zu); lower ty", pl.smem, d.smem_optin);
+    pl.nitems = pl.ntile * t.nchunk;
+    pl.tma_ok = true;
+    *out = pl;
+    return MG_OK;
+}
+
+// deepest tile that fits the block and shared memory; z chunks to give
+// every SM about one item (one CTA per SM)
+static mg_tiling fh_default_tiling(const Geometry& g, const DevInfo& d)
+{
+    if (!fh_shape_ok(g)) return mg_tiling{1, 1, 4, 1};
+    int ty = 1;
+    if (!g.flat)
+        for (int t = std::min(g.lny, kFhBlock / (g.lnx / 4) - 2); t >= 1; --t) {
+            TilePlan pl;
+            if (plan_fh_tiling(g, mg_tiling{t, 1, 3, 0}, d, &pl) == MG_OK) {
+                ty = t;
+                break;
+            }
+            clear_error();
+        }
+    const int ntile = g.flat ? 1 : (g.lny + ty - 1) / ty;
+    int nchunk = std::max(1, d.sms / ntile);
+    nchunk = std::min(nchunk, std::max(1, g.lnz / 8));
+    if (nchunk > 1 && (nchunk & 1)) nchunk -= 1;
+    return mg_tiling{ty, nchunk, 3, 0};
+}
+
 template <typename T, bool FLAT, bool SIMPLE, bool MASS>
 static StepKernel pick_nbuf(int nbuf)
 {
@@ -288,8 +364,31 @@ static StepKernel pick_shape(bool flat, bool simple, int nbuf, int block)
     return simple ? pick_maxt<T, false, true, MASS>(nbuf, block) : pick_maxt<T, false, false, MASS>(nbuf, block);
 }
 
+// stage order of the march kernels (MG_MARCH_ORDER=0: barrier between the
+// stages, as ch_step_kernel); MG_MARCH=0 selects the earlier kernels
+static int march_order()
+{
+    static const int v = [] {
+        const char* e = std::getenv("MG_MARCH_ORDER");
+        return e && e[0] == '0' ? 0 : 1;
+    }();
+    return v;
+}
+static bool march_enabled()
+{
+    static const bool v = [] {
+        const char* e = std::getenv("MG_MARCH");
+        return !(e && e[0] == '0');
+    }();
+    return v;
+}
+
 StepKernel step_kernel(bool fp32, bool flat, int nbuf, bool simple, int block, bool mass, int nx)
 {
+    if (simple && !flat && nx > 0 && march_enabled()) {
+        StepKernel k = fp32 ? march_kernel_f32(nx, nbuf, mass, march_order()) : march_kernel_f64(nx, nbuf, march_order());
+        if (k) return k;
+    }
     if (fp32 && simple && !flat && nx > 0) {
         StepKernel k = mass ? pick_lean<true>(nx, nbuf) : pick_lean<false>(nx, nbuf);
         if (k) return k;
@@ -305,6 +404,11 @@ StepKernel step_kernel(bool fp32, bool flat, int nbuf, bool simple, int block, b
 }
 
 bool nbuf_ok(int nbuf) { return nbuf == 3 || nbuf == 4 || nbuf == 6 || nbuf == 8; }
+
+bool march_batch_job(const Geometry& g)
+{
+    return march_enabled() && geometry_simple(g) && !g.flat && tma_shape_ok(g) && march_batch_width(g.es, g.lnx);
+}
 
 int prepare_kernels(const DevInfo& d)
 {
@@ -323,6 +427,16 @@ int prepare_kernels(const DevInfo& d)
                                 MG_CUDA(cudaFuncSetAttribute(step_kernel(f32, fl, nb, sm, bl, ms && f32, fx),
                                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                              (int)d.smem_optin));
+    MG_CUDA(cudaFuncSetAttribute(fh_march_kernel<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));
+    MG_CUDA(cudaFuncSetAttribute(fh_march_kernel<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));
+    for (int nb : {3, 6})
+        for (int ms = 0; ms < 2; ++ms) {
+            MG_CUDA(cudaFuncSetAttribute(march_batch_kernel_f32(nb, ms), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)d.smem_optin));
+            if (!ms)
+                MG_CUDA(cudaFuncSetAttribute(march_batch_kernel_f64(nb), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)d.smem_optin));
+        }
     done = true;
     return MG_OK;
 }
@@ -660,9 +774,16 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const Fh
     if (fh && (p.precision != MG_FP64 || p.mass_correct))
         return fail(MG_EINVAL, "the variable-mobility model runs in FP64 without mass feedback");
     MG_CUDA(cudaSetDevice(device));
-    if (fh) j->tiling = mg_tiling{1, 1, 4, 1};  // the per-site path
-    else j->tiling = batch_tiling ? batch_tiling_for(j->g, info, device, batch_threads, batch_planes) : default_tiling(j->g, info, device);
-    MG_TRY(plan_tiling(j->g, j->tiling, info, &j->plan));
+    if (fh) {
+        // the fused variable-mobility kernel where the shape allows, else the
+        // per-site path (path 1)
+        j->tiling = fh_default_tiling(j->g, info);
+        MG_TRY(plan_fh_tiling(j->g, j->tiling, info, &j->plan));
+    } else {
+        j->tiling = batch_tiling ? batch_tiling_for(j->g, info, device, batch_threads, batch_planes)
+                                 : default_tiling(j->g, info, device);
+        MG_TRY(plan_tiling(j->g, j->tiling, info, &j->plan));
+    }
     if (j->p.mass_correct && !j->plan.tma_ok)
         return fail(MG_EINVAL, "mass_correct needs a shape the tiled kernel takes (nx multiple of %d)", 32);
     j->target = target;
@@ -739,9 +860,9 @@ void Engine::remove_job(Job* j)
 
 int Engine::set_tiling(Job* j, const mg_tiling& t)
 {
-    if (j->d_fh && t.path != 1) return fail(MG_EINVAL, "the variable-mobility model runs on the per-site path (path 1)");
     TilePlan pl;
-    MG_TRY(plan_tiling(j->g, t, info, &pl));
+    if (j->d_fh) MG_TRY(plan_fh_tiling(j->g, t, info, &pl));
+    else MG_TRY(plan_tiling(j->g, t, info, &pl));
     if (j->p.mass_correct && !pl.tma_ok) return fail(MG_EINVAL, "mass_correct needs the tiled kernel");
     MG_CUDA(cudaStreamSynchronize(stream));
     long long* part = nullptr;
@@ -809,6 +930,16 @@ void Engine::free_graveyard()
     graveyard_.clear();
 }
 
+StepKernel Engine::group_kernel(const Group& g) const
+{
+    if (g.fhm) return g.flat ? fh_march_kernel<3, true> : fh_march_kernel<3, false>;
+    if (g.mbatch) {
+        StepKernel k = g.fp32 ? march_batch_kernel_f32(g.nbuf, g.mass) : march_batch_kernel_f64(g.nbuf);
+        if (k) return k;
+    }
+    return step_kernel(g.fp32, g.flat, g.nbuf, g.simple, g.block, g.mass, g.fixed_nx);
+}
+
 int Engine::rebuild()
 {
     ++rebuilds_;
@@ -822,8 +953,8 @@ int Engine::rebuild()
     // results, stay as chosen.
     if (jobs.size() > 1)
         for (Job* j : jobs) {
-            if (!j->plan.tma_ok) continue;
-            const int nb = j->g.flat ? 8 : 4;
+            if (!j->plan.tma_ok || j->d_fh) continue;
+            const int nb = j->g.flat ? 8 : (march_batch_job(j->g) ? kMarchBatchNbuf : 4);
             if (j->tiling.nbuf == nb) continue;
             mg_tiling t = j->tiling;
             t.nbuf = nb;
@@ -843,7 +974,16 @@ int Engine::rebuild()
     // class; a class whose planes together outgrow shared memory is split;
     // generic jobs run on their own
     std::map<long long, std::vector<Group>> by_key;
+    std::map<int, Group> fh_groups;  // fused variable-mobility jobs by flatness
     for (Job* j : jobs) {
+        if (j->d_fh && j->plan.tma_ok) {
+            Group& g = fh_groups[j->g.flat ? 1 : 0];
+            g.fhm = true;
+            g.flat = j->g.flat;
+            g.nbuf = j->tiling.nbuf;
+            g.jobs.push_back(j);
+            continue;
+        }
         if (!j->plan.tma_ok) {
             Group g;
             g.generic = true;
@@ -854,7 +994,9 @@ int Engine::rebuild()
         }
         const bool simple = geometry_simple(j->g);
         const bool mass = j->p.mass_correct && j->g.es == 4;
-        const int fixed = fixed_width_kernel(j->g, j->tiling.nbuf) ? j->g.lnx : 0;
+        // several jobs of march widths: one launch for all widths (-1)
+        const bool mb = jobs.size() > 1 && march_batch_job(j->g) && j->tiling.nbuf == kMarchBatchNbuf;
+        const int fixed = mb ? -1 : (fixed_width_kernel(j->g, j->tiling.nbuf) ? j->g.lnx : 0);
         const long long key = (long long)((j->g.es == 4 ? 1 : 0) | (j->g.flat ? 2 : 0) | (simple ? 4 : 0) |
                                           (mass ? 8 : 0) | (j->tiling.nbuf << 4)) |
                               ((long long)fixed << 12);
@@ -879,6 +1021,7 @@ int Engine::rebuild()
             g.mplane = 0;
             groups_.push_back(g);
         }
+    for (auto& kv : fh_groups) groups_.push_back(kv.second);
     for (Group& g : groups_) {
         if (g.generic) continue;
         std::vector<int> begin, slot;
@@ -896,11 +1039,14 @@ int Engine::rebuild()
         g.fixed_nx = g.jobs.front()->g.lnx;
         for (Job* j : g.jobs)
             if (j->g.lnx != g.fixed_nx) g.fixed_nx = 0;
-        g.smem = group_smem(g.nbuf, g.cplane, g.mplane, g.fp32 ? 4 : 8);
+        g.mbatch = !g.fhm && jobs.size() > 1 && g.simple && !g.flat && g.nbuf == kMarchBatchNbuf;
+        for (Job* j : g.jobs)
+            if (!march_batch_job(j->g)) g.mbatch = false;
+        g.smem = g.fhm ? fh_smem(g.nbuf, g.cplane, g.mplane) : group_smem(g.nbuf, g.cplane, g.mplane, g.fp32 ? 4 : 8);
         if (g.smem > info.smem_optin) return fail(MG_EINVAL, "batch group needs %zu bytes of shared memory", g.smem);
         int occ = 1;
         MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &occ, step_kernel(g.fp32, g.flat, g.nbuf, g.simple, g.block, g.mass, g.fixed_nx), g.block, g.smem));
+            &occ, group_kernel(g), g.block, g.smem));
         occ = std::max(occ, 1);
         g.grid = std::min(items, info.sms * occ);
         MG_CUDA(cudaMalloc(&g.d_item_begin, sizeof(int) * begin.size()));
@@ -973,7 +1119,7 @@ int Engine::launch_lane(const Group& g, Job* generic_job, cudaStream_t st)
         a.spin_limit = spin_limit();
         a.err = d_err_;
         a.tx_extra = fault_tx_extra();
-        step_kernel(g.fp32, g.flat, g.nbuf, g.simple, g.block, g.mass, g.fixed_nx)<<<g.grid, g.block, g.smem, st>>>(a);
+        group_kernel(g)<<<g.grid, g.block, g.smem, st>>>(a);
     }
     // the noise term, per job that has one, after the step
     auto noise = [&](Job* j) {
@@ -983,7 +1129,7 @@ int Engine::launch_lane(const Group& g, Job* generic_job, cudaStream_t st)
         else ch_noise_kernel<double><<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
     };
     if (g.generic) noise(generic_job);
-    else
+    else if (!g.fhm)  // the fused variable-mobility kernel adds its noise itself
         for (Job* j : g.jobs) noise(j);
     MG_CUDA(cudaGetLastError());
     return MG_OK;
@@ -1204,7 +1350,12 @@ int Engine::mobility(Job* j, double* host)
     if (!host) return fail(MG_EINVAL, "null field");
     if (!j->d_fh) return fail(MG_EINVAL, "not a variable-mobility job");
     MG_TRY(sync(-1));
-    MG_CUDA(cudaMemcpy(host, j->d_mob, j->g.n * sizeof(double), cudaMemcpyDeviceToHost));
+    // recomputed from the input of the last step, which the other ping-pong
+    // buffer still holds (the fused kernel keeps the mobility on chip)
+    fh_mobility_kernel<<<4 * info.sms, 256, 0, stream>>>(d_jobs_ + j->slot, j->d_mob);
+    MG_CUDA(cudaGetLastError());
+    MG_CUDA(cudaMemcpyAsync(host, j->d_mob, j->g.n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    MG_CUDA(cudaStreamSynchronize(stream));
     return MG_OK;
 }
 

@@ -36,6 +36,8 @@ const char* last_error();
         if (rc_ != MG_OK) return rc_; \
     } while (0)
 
+using StepKernel = void (*)(StepArgs);
+
 struct DevInfo {
     int sms = 0;
     size_t smem_optin = 0;
@@ -65,9 +67,14 @@ struct TilePlan {
     int ntile = 0, nitems = 0;
 };
 int plan_tiling(const Geometry& g, const mg_tiling& t, const DevInfo& d, TilePlan* out);
+int plan_fh_tiling(const Geometry& g, const mg_tiling& t, const DevInfo& d, TilePlan* out);
+bool fh_shape_ok(const Geometry& g);
 bool tma_shape_ok(const Geometry& g);
 mg_tiling default_tiling(const Geometry& g, const DevInfo& d, int device);
 std::string tune_key(const Geometry& g);
+// tiling of a job that shares launches: CTAs of about `threads` threads,
+// z-chunks of about `planes` planes
+mg_tiling batch_tiling_for(const Geometry& g, const DevInfo& d, int device, int threads, int planes);
 bool tune_lookup(const std::string& key, mg_tiling* t);
 void tune_store(const std::string& key, const mg_tiling& t, double ms);
 
@@ -143,6 +150,8 @@ class Engine {
    private:
     struct Group {
         bool fp32 = false, flat = false, generic = false, simple = false, mass = false;
+        bool mbatch = false;  // ch_march_batch_kernel: jobs of any march width
+        bool fhm = false;     // fh_march_kernel: fused variable-mobility jobs
         int nbuf = 4;
         std::vector<Job*> jobs;
         int nitems = 0, grid = 0, block = 0;
@@ -153,6 +162,7 @@ class Engine {
         int* d_slot = nullptr;
     };
     int rebuild();
+    StepKernel group_kernel(const Group& g) const;
     void free_groups();
     int launch_lane(const Group& g, Job* generic_job, cudaStream_t st);
     int launch_steps(int k);
@@ -189,9 +199,19 @@ class Engine {
 };
 
 // kernel table
-using StepKernel = void (*)(StepArgs);
 StepKernel step_kernel(bool fp32, bool flat, int nbuf, bool simple, int block, bool mass, int nx = 0);
 bool nbuf_ok(int nbuf);
+// march step kernels (ch_march.cuh; march_f32.cu, march_f64.cu): periodic,
+// equal spacing, 3-D, row widths up to 256, ring depths 3, 4, 6; nullptr
+// where no variant exists.  order 1 runs both stages between two barriers.
+StepKernel march_kernel_f32(int nx, int nbuf, bool mass, int order);
+StepKernel march_kernel_f64(int nx, int nbuf, int order);
+// one launch for jobs of every march width (ring depths 3 and 6)
+StepKernel march_batch_kernel_f32(int nbuf, bool mass);
+StepKernel march_batch_kernel_f64(int nbuf);
+bool march_batch_job(const Geometry& g);  // a job the batch kernel takes
+// ring depth of march jobs that share launches (batch, server)
+constexpr int kMarchBatchNbuf = 6;
 bool geometry_simple(const Geometry& g);
 bool fixed_width_kernel(const Geometry& g, int nbuf);
 int prepare_kernels(const DevInfo& d);

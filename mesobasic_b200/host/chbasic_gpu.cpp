@@ -33,7 +33,7 @@ CHBasicGPU::CHBasicGPU(const CommonParams& pin, const InputFile& in) : p(pin)
     const std::string prec = in("PFApp/precision", "fp64");
     if (prec != "fp64" && prec != "fp32") throw std::invalid_argument("PFApp/precision must be fp64 or fp32");
     gp.precision = prec == "fp32" ? MG_FP32 : MG_FP64;
-    gp.mass_correct = gp.precision == MG_FP32 ? in("PFApp/mass_correct", 4) : 0;
+    gp.mass_correct = gp.precision == MG_FP32 ? in("PFApp/mass_correct", 1) : 0;
     // the reference's per-step fluctuation term (TIPSphil.cpp:200-209); off
     // by default in the plain Cahn-Hilliard model
     gp.noise = in("PFApp/noiseStr", 0.0);

@@ -17,7 +17,7 @@
 //   dump_prefix    also write raw dumps <prefix>_<step>.rank0   (none)
 // Keys of this build only:
 //   precision      fp64 (bit-identical to the reference build) | fp32   fp64
-//   mass_correct   fp32: FP64 mass feedback every K-th step (0 off) 4
+//   mass_correct   fp32: FP64 mass feedback every K-th step (0 off) 1
 //   noiseStr       per-step noise c += dt*noiseStr*(u - 0.5)       0 (off)
 //   noise_seed     key of the noise generator                      seed
 //   device         CUDA device                                     0

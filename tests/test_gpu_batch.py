@@ -52,6 +52,33 @@ def test_batch_equals_standalone_bitwise():
         b.close()
 
 
+def test_c4_style_batch_is_one_launch_and_autotune_keeps_results():
+    """FP32 cubic jobs of mixed march widths (64..192) step in ONE persistent
+    launch per step; re-tiling the batch by the autotuner between steps
+    leaves every job bit-identical to its standalone run."""
+    rng = np.random.default_rng(3)
+    jobs = []
+    for j, e in enumerate((64, 96, 128, 160, 192, 64, 128)):
+        p = mb.make_params(e, e, e, 0.005, kappa=float(rng.uniform(0.5, 2.0)), precision="fp32")
+        jobs.append((p, mb.ic_generate((e, e, e), float(rng.uniform(-0.4, 0.4)), 0.05, False, 2000 + j)))
+    b = mb.Batch([p for p, _ in jobs])
+    try:
+        for i, (_, ic) in enumerate(jobs):
+            b.set_field(i, ic)
+        b.step(12)
+        assert b.info()["launches_per_step"] == 1
+        tuned = b.autotune(trials=2)
+        assert tuned["threads"] > 0 and tuned["planes"] > 0 and tuned["ms_per_step"] > 0
+        b.step(13)
+        assert b.info()["launches_per_step"] == 1
+        for i, (p, ic) in enumerate(jobs):
+            want, st = alone(p, ic, 25)
+            assert np.array_equal(b.get_field(i), want), i
+            assert b.reduce(i)["step"] == 25
+    finally:
+        b.close()
+
+
 def test_batch_fp64_job_matches_oracle(oracle):
     p = mb.make_params(64, 32, 24, 0.005, kappa=1.3)
     q = mb.make_params(96, 96, 1, 0.01)
