@@ -1205,7 +1205,7 @@ int Engine::enqueue_steps(int nsteps)
     MG_CUDA(cudaSetDevice(device));
     if (dirty_) MG_TRY(rebuild());
     if (jobs.empty()) return MG_OK;
-    const int gk = graph_steps();
+    const int gk = graph_max_steps > 0 ? std::min(graph_max_steps, graph_steps()) : graph_steps();
     while (nsteps > 0) {
         if (gk >= 2 && nsteps >= 2) {
             const int k = std::min(nsteps, gk);

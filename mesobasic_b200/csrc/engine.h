@@ -142,6 +142,10 @@ class Engine {
     // spread each job over the SMs
     int batch_threads = 320;
     int batch_planes = 128;
+    // longest CUDA graph captured (0: the default of 50 steps).  An engine
+    // whose job set changes often (the server) captures short graphs and
+    // replays them back to back: each change costs one short capture.
+    int graph_max_steps = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;  // created on first use (download_finished)
     DevInfo info;

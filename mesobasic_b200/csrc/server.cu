@@ -3,7 +3,8 @@
 //
 // A worker thread owns one Engine.  Each tick it
 //   1. admits queued jobs, oldest first, that fit the HBM budget and a free
-//      slot (first fit: a large job at the head does not block small ones);
+//      slot (first fit: a large job at the head does not block small ones),
+//      with their allocation and upload outside the server lock;
 //   2. enqueues steps_per_tick steps for every admitted job together -- one
 //      fused launch per class per step, all jobs' tiles in the same
 //      persistent grid, classes side by side on their own streams; a job
@@ -75,7 +76,7 @@ struct mg_server {
     long long ticks = 0;
 
     void run();
-    void admit_locked();
+    void admit();
     void retire(ServerJob* sj, bool ok, const char* why);
 };
 
@@ -85,36 +86,61 @@ static size_t job_bytes(const mg_ch_params& p)
     return 2 * n * (p.precision == MG_FP32 ? 4 : 8) + (1 << 16);
 }
 
-void mg_server::admit_locked()
+// Admission.  Under the lock, the queue is scanned first fit in arrival
+// order for jobs that fit the HBM budget and a free slot; they are reserved
+// (their bytes counted, taken off the queue).  The device work -- buffers,
+// tensor maps, upload of the initial field -- runs after the lock is
+// released: only the worker thread touches the engine, so submitters never
+// wait for an allocation or a copy.
+void mg_server::admit()
 {
-    for (auto it = queue.begin(); it != queue.end();) {
-        if ((int)running.size() >= max_inflight) break;
-        ServerJob* sj = *it;
-        if ((double)(in_use + sj->bytes) > budget) {
-            ++it;
-            continue;
+    std::vector<ServerJob*> take;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        for (auto it = queue.begin(); it != queue.end();) {
+            if ((int)(running.size() + take.size()) >= max_inflight) break;
+            ServerJob* sj = *it;
+            if ((double)(in_use + sj->bytes) > budget) {
+                ++it;
+                continue;
+            }
+            in_use += sj->bytes;
+            peak = std::max(peak, in_use);
+            take.push_back(sj);
+            it = queue.erase(it);
         }
+    }
+    if (take.empty()) return;
+    std::vector<ServerJob*> ok, bad;
+    std::vector<std::string> why;
+    for (ServerJob* sj : take) {
         mg::Job* j = nullptr;
         int rc = eng.add_job(sj->p, sj->nsteps, &j);
         if (rc == MG_OK) rc = eng.upload(j, sj->ic.data(), sj->nsteps);
         if (rc != MG_OK) {
             if (j) eng.remove_job(j);
-            sj->state = MG_JOB_FAILED;
-            sj->error = mg::last_error();
-            sj->t_done = Clock::now();
-            ++failed;
-            it = queue.erase(it);
-            cv_done.notify_all();
+            bad.push_back(sj);
+            why.push_back(mg::last_error());
             continue;
         }
         std::vector<double>().swap(sj->ic);
         sj->job = j;
-        sj->state = MG_JOB_RUNNING;
-        in_use += sj->bytes;
-        peak = std::max(peak, in_use);
-        running.push_back(sj);
-        it = queue.erase(it);
+        ok.push_back(sj);
     }
+    std::lock_guard<std::mutex> lock(mu);
+    for (ServerJob* sj : ok) {
+        sj->state = MG_JOB_RUNNING;
+        running.push_back(sj);
+    }
+    for (size_t i = 0; i < bad.size(); ++i) {
+        ServerJob* sj = bad[i];
+        in_use -= sj->bytes;
+        sj->state = MG_JOB_FAILED;
+        sj->error = why[i];
+        sj->t_done = Clock::now();
+        ++failed;
+    }
+    if (!bad.empty()) cv_done.notify_all();
 }
 
 void mg_server::retire(ServerJob* sj, bool ok, const char* why)
@@ -167,18 +193,15 @@ void mg_server::run()
     // and diagnostics read on a side stream) while the next tick runs
     std::vector<ServerJob*> finished;
     for (;;) {
-        {
-            std::unique_lock<std::mutex> lock(mu);
+        for (;;) {
             auto t0 = Clock::now();
-            admit_locked();
-            admit_s += seconds_since(t0);
-            while (running.empty()) {
-                if (stopping && queue.empty()) return;
-                cv_work.wait_for(lock, std::chrono::milliseconds(20));
-                t0 = Clock::now();
-                admit_locked();
-                admit_s += seconds_since(t0);
-            }
+            admit();
+            const double as = seconds_since(t0);
+            std::unique_lock<std::mutex> lock(mu);
+            admit_s += as;
+            if (!running.empty()) break;
+            if (stopping && queue.empty()) return;
+            cv_work.wait_for(lock, std::chrono::milliseconds(20));
         }
         const long long k = steps_per_tick;
         // steps only when some admitted job still has steps to take
@@ -229,6 +252,9 @@ int mg_server_create(int device, double hbm_budget_gb, int max_jobs_in_flight, i
     // (four settings measured back to back on one B200)
     s->eng.batch_threads = mg::mg_env_int("MG_SERVER_THREADS", 320);
     s->eng.batch_planes = mg::mg_env_int("MG_SERVER_PLANES", 64);
+    // admissions and retirements change the job set between ticks: short
+    // graphs keep the recapture after each change cheap
+    s->eng.graph_max_steps = mg::mg_env_int("MG_SERVER_GRAPH_STEPS", 10);
     s->budget = hbm_budget_gb * 1e9;
     s->max_inflight = max_jobs_in_flight;
     s->steps_per_tick = steps_per_tick > 0 ? steps_per_tick : 100;
