@@ -128,3 +128,26 @@ def test_noalloc_rejects_tall_2d_field_on_the_host():
     assert rc == _lib.MG_EINVAL
     msg = L.mg_last_error()
     assert b"5000 planes" in msg and b"ny of a 2-D field" in msg and b"at most 4096" in msg
+
+
+def test_create_returns_a_status_without_crashing():
+    """mg_ch_create / mg_batch_create build an engine on the host before any
+    device call: on a machine without a GPU they return MG_ECUDA or MG_EINVAL
+    (with a GPU, MG_OK), never crash.  Guards against objects built against
+    different layouts of the engine's classes."""
+    import ctypes
+    import mesobasic_b200 as mb
+    from mesobasic_b200 import _lib
+    L = _lib.load()
+    p = mb.make_params(32, 16, 8, 0.005)
+    h = ctypes.c_void_p()
+    rc = L.mg_ch_create(ctypes.byref(p), 0, ctypes.byref(h))
+    assert rc in (_lib.MG_OK, _lib.MG_ECUDA, _lib.MG_EINVAL), rc
+    if rc == _lib.MG_OK:
+        L.mg_ch_destroy(h)
+    arr = (_lib.Params * 2)(p, mb.make_params(64, 64, 64, 0.005, precision="fp32"))
+    b = ctypes.c_void_p()
+    rc = L.mg_batch_create(arr, 2, 0, ctypes.byref(b))
+    assert rc in (_lib.MG_OK, _lib.MG_ECUDA, _lib.MG_EINVAL), rc
+    if rc == _lib.MG_OK:
+        L.mg_batch_destroy(b)
