@@ -385,7 +385,7 @@ def run_serve(mb, dev, window_s, seed=11, rate=20.0, burst=0):
             "gbs": st["site_updates_per_s"] * upd_bytes / upd / 1e9,
             "mean_ms": st["mean_ms"], "completed": st["completed"], "failed": st["failed"],
             "worker_s": {k: st[k] for k in ("step_s", "admit_s", "retire_s")},
-            "ticks": st["ticks"], "rebuilds": st["rebuilds"],
+            "ticks": st["ticks"], "rebuilds": st["rebuilds"], "refreshes": st["refreshes"],
             "glups": st["site_updates_per_s"] / 1e9, "hbm_peak_gb": st["hbm_peak_gb"], "wall_s": wall,
             "submitted": len(arrivals),
             "workload": (f"{burst} jobs submitted at once (seed {seed})" if burst else
@@ -505,7 +505,7 @@ def run_ours(args, rank, world, local_rank):
             # saturated: a burst of the same mix, the queue never empty
             sat = run_serve(mb, dev, args.serve_seconds, burst=args.serve_burst)
             serve["saturated"] = {k: sat[k] for k in ("glups", "sims_per_hour", "p50_ms", "p99_ms", "completed",
-                                                      "ticks", "rebuilds", "wall_s")}
+                                                      "ticks", "rebuilds", "refreshes", "wall_s")}
             # the fraction uses the mix's algorithmic bytes (8 B per FP32
             # site update, 16 B per FP64)
             serve["saturated"]["roofline_frac"] = sat["gbs"] / peak

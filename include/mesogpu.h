@@ -313,10 +313,11 @@ typedef struct {
     double hbm_in_use_gb, hbm_peak_gb;
     /* where the worker thread's time went: enqueueing and waiting for step
        ticks (GPU busy), admitting jobs (allocation, upload), retiring jobs
-       (download, diagnostics); ticks run and launch-set rebuilds (each
-       recaptures the step graph) */
+       (download, diagnostics); ticks run, launch-set rebuilds (each
+       recaptures the step graph) and job-set changes absorbed without one
+       (the launch lanes' device tables rewritten, the graphs kept) */
     double step_s, admit_s, retire_s;
-    long long ticks, rebuilds;
+    long long ticks, rebuilds, refreshes;
 } mg_server_stats;
 
 #define MG_JOB_QUEUED 0

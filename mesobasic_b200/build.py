@@ -67,7 +67,12 @@ def build(verbose: bool = False, force: bool = False) -> str:
 
     def compile_one(job):
         src, flags = job
+        import time
+        t0 = time.time()
         out = _run(flags, verbose)
+        # stamp the object with the time its compile started: a source or
+        # header edited while it compiled stays newer, so it is rebuilt
+        os.utime(flags[flags.index("-o") + 1], (t0, t0))
         with open(os.path.join(BUILD, src + ".ptxas.txt"), "w") as f:  # registers / spills per kernel
             f.write(out)
         return out

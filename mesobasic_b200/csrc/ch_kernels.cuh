@@ -40,6 +40,7 @@ namespace mg {
 template <typename T, int NBUF, bool FLAT, bool SIMPLE, bool MASS, int NXC = 0>
 __global__ void __launch_bounds__(NXC ? kMaxBlock : kMaxBlockGeneric, 1) ch_step_kernel(StepArgs a)
 {
+    step_counts(a);
     constexpr int W = Strip<T>::W;  // elements per thread strip
     constexpr bool PAIRS = (sizeof(T) == 4) && SIMPLE;
     using A = Arith<T>;

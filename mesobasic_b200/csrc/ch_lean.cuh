@@ -20,6 +20,7 @@ namespace mg {
 template <int NXC, int NBUF, bool MASS>
 __global__ void __launch_bounds__(kMaxBlock, 1) ch_lean_kernel(StepArgs a)
 {
+    step_counts(a);
     constexpr int W = 8, HW = 4;
     constexpr int NQ = NXC / W;  // threads per row
     static_assert(NXC % W == 0 && NXC <= 256 && NQ <= 32 && (NQ & (NQ - 1)) == 0,

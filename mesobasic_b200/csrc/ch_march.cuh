@@ -458,6 +458,7 @@ __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int loc
 template <typename T, int NXC, int NBUF, bool MASS, int ORDER>
 __global__ void __launch_bounds__(kMaxBlock, 1) ch_march_kernel(StepArgs a)
 {
+    step_counts(a);
     MarchCta cta = march_setup<NBUF>(a, sizeof(T));
     for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
         const int j = find_job(a.item_begin, a.njobs, item);
@@ -485,6 +486,7 @@ __device__ __noinline__ uint32_t march_item_call(StepArgs a, JobDev* J, int loca
 template <typename T, int NBUF, bool MASS>
 __global__ void __launch_bounds__(kMaxBlock, 1) ch_march_batch_kernel(StepArgs a)
 {
+    step_counts(a);
     MarchCta cta = march_setup<NBUF>(a, sizeof(T));
     uint32_t ph = cta.ph;
     for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {

@@ -127,7 +127,21 @@ struct StepArgs {
     int* err;               // launch-wide error word (max of DeviceError)
     uint32_t tx_extra;      // test hook: bytes expected beyond a plane (0 in use);
                             // nonzero makes every TMA wait run out
+    const int* counts;      // non-null: device [njobs, nitems] read at kernel
+                            // start in place of the two fields above (lanes
+                            // whose job list is rewritten between graph replays)
 };
+
+#ifdef __CUDACC__
+// the launch's job and item counts (StepArgs::counts, else the fields)
+__device__ __forceinline__ void step_counts(StepArgs& a)
+{
+    if (a.counts) {
+        a.njobs = __ldg(a.counts);
+        a.nitems = __ldg(a.counts + 1);
+    }
+}
+#endif
 
 // Shared-memory header: NBUF mbarriers, broadcast words, reduction scratch.
 struct SmemHead {

@@ -914,6 +914,7 @@ void Engine::free_groups()
     for (Group& g : groups_) {
         cudaFree(g.d_item_begin);
         cudaFree(g.d_slot);
+        cudaFree(g.d_counts);
     }
     groups_.clear();
 }
@@ -940,18 +941,85 @@ StepKernel Engine::group_kernel(const Group& g) const
     return step_kernel(g.fp32, g.flat, g.nbuf, g.simple, g.block, g.mass, g.fixed_nx);
 }
 
+// The job list, item offsets and (stable lanes) counts of a group, written
+// to its device tables.
+int Engine::write_tables(const Group& g)
+{
+    std::vector<int> begin, slot;
+    int items = 0;
+    for (Job* j : g.jobs) {
+        begin.push_back(items);
+        slot.push_back(j->slot);
+        items += j->plan.nitems;
+    }
+    begin.push_back(items);
+    if ((int)slot.size() > g.table_cap) return fail(MG_EINVAL, "launch table holds %d jobs, not %zu", g.table_cap, slot.size());
+    MG_CUDA(cudaMemcpy(g.d_item_begin, begin.data(), sizeof(int) * begin.size(), cudaMemcpyHostToDevice));
+    if (!slot.empty()) MG_CUDA(cudaMemcpy(g.d_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice));
+    if (g.d_counts) {
+        const int counts[2] = {(int)g.jobs.size(), items};
+        MG_CUDA(cudaMemcpy(g.d_counts, counts, sizeof counts, cudaMemcpyHostToDevice));
+    }
+    return MG_OK;
+}
+
+// Maps the new groups onto the current stable lanes: every new group needs a
+// lane of the same kernel whose block and planes hold its tiles; lanes left
+// without a group run empty (their CTAs find no item).  Lanes that bake a
+// job into the graph (per-site jobs, noise launches) rule the refresh out.
+bool Engine::refresh_tables(std::vector<Group>& ng)
+{
+    if (groups_.empty()) return false;
+    auto bakes_jobs = [](const Group& g) {
+        if (g.generic) return true;
+        for (Job* j : g.jobs)
+            if (j->p.noise > 0 && !g.fhm) return true;
+        return false;
+    };
+    for (const Group& l : groups_)
+        if (bakes_jobs(l) || !l.d_counts) return false;
+    std::vector<int> lane_of(ng.size(), -1);
+    std::vector<bool> used(groups_.size(), false);
+    for (size_t i = 0; i < ng.size(); ++i) {
+        const Group& g = ng[i];
+        if (bakes_jobs(g)) return false;
+        for (size_t l = 0; l < groups_.size(); ++l) {
+            const Group& L = groups_[l];
+            if (used[l] || L.key != g.key || L.sub != g.sub || group_kernel(L) != group_kernel(g)) continue;
+            if (g.block > L.block || g.cplane > L.cplane || g.mplane > L.mplane) return false;
+            lane_of[i] = (int)l;
+            used[l] = true;
+            break;
+        }
+        if (lane_of[i] < 0) return false;
+    }
+    for (size_t l = 0; l < groups_.size(); ++l) {
+        groups_[l].jobs.clear();
+        groups_[l].nitems = 0;
+    }
+    for (size_t i = 0; i < ng.size(); ++i) {
+        Group& L = groups_[lane_of[i]];
+        L.jobs = ng[i].jobs;
+        L.nitems = ng[i].nitems;
+    }
+    for (const Group& L : groups_)
+        if (write_tables(L) != MG_OK) {
+            clear_error();
+            return false;
+        }
+    return true;
+}
+
 int Engine::rebuild()
 {
-    ++rebuilds_;
     MG_CUDA(cudaStreamSynchronize(stream));
     free_graveyard();
-    drop_graphs();
-    free_groups();
     // Several jobs: one ring depth per class (4 planes for 3-D jobs, 8 for
     // 2-D) so that each class steps in one launch.  Only nbuf changes; the
     // tile rows and z chunks, which fix a job's reduction order and so its
     // results, stay as chosen.
-    if (jobs.size() > 1)
+    const bool shared = jobs.size() > 1 || stable_lanes;  // launches shared by several jobs
+    if (shared)
         for (Job* j : jobs) {
             if (!j->plan.tma_ok || j->d_fh) continue;
             const int nb = j->g.flat ? 8 : (march_batch_job(j->g) ? kMarchBatchNbuf : 4);
@@ -973,11 +1041,13 @@ int Engine::rebuild()
     // one launch per (precision, flat, simple, mass, nbuf, row-width kernel)
     // class; a class whose planes together outgrow shared memory is split;
     // generic jobs run on their own
+    std::vector<Group> ng;  // the new launch groups
     std::map<long long, std::vector<Group>> by_key;
     std::map<int, Group> fh_groups;  // fused variable-mobility jobs by flatness
     for (Job* j : jobs) {
         if (j->d_fh && j->plan.tma_ok) {
             Group& g = fh_groups[j->g.flat ? 1 : 0];
+            g.key = -1 - (j->g.flat ? 1 : 0);
             g.fhm = true;
             g.flat = j->g.flat;
             g.nbuf = j->tiling.nbuf;
@@ -989,13 +1059,13 @@ int Engine::rebuild()
             g.generic = true;
             g.fp32 = j->g.es == 4;
             g.jobs.push_back(j);
-            groups_.push_back(g);
+            ng.push_back(g);
             continue;
         }
         const bool simple = geometry_simple(j->g);
         const bool mass = j->p.mass_correct && j->g.es == 4;
         // several jobs of march widths: one launch for all widths (-1)
-        const bool mb = jobs.size() > 1 && march_batch_job(j->g) && j->tiling.nbuf == kMarchBatchNbuf;
+        const bool mb = shared && march_batch_job(j->g) && j->tiling.nbuf == kMarchBatchNbuf;
         const int fixed = mb ? -1 : (fixed_width_kernel(j->g, j->tiling.nbuf) ? j->g.lnx : 0);
         const long long key = (long long)((j->g.es == 4 ? 1 : 0) | (j->g.flat ? 2 : 0) | (simple ? 4 : 0) |
                                           (mass ? 8 : 0) | (j->tiling.nbuf << 4)) |
@@ -1006,6 +1076,8 @@ int Engine::rebuild()
                                      std::max(gs.back().mplane, j->plan.mplane), es) > info.smem_optin)
             gs.emplace_back();
         Group& g = gs.back();
+        g.key = key;
+        g.sub = (int)gs.size() - 1;
         g.fp32 = j->g.es == 4;
         g.flat = j->g.flat;
         g.simple = simple;
@@ -1019,40 +1091,62 @@ int Engine::rebuild()
         for (Group& g : kv.second) {
             g.cplane = 0;
             g.mplane = 0;
-            groups_.push_back(g);
+            ng.push_back(g);
         }
-    for (auto& kv : fh_groups) groups_.push_back(kv.second);
-    for (Group& g : groups_) {
+    for (auto& kv : fh_groups) ng.push_back(kv.second);
+    for (Group& g : ng) {
         if (g.generic) continue;
-        std::vector<int> begin, slot;
         int items = 0;
         for (Job* j : g.jobs) {
-            begin.push_back(items);
-            slot.push_back(j->slot);
             items += j->plan.nitems;
             g.block = std::max(g.block, j->plan.block);
             g.cplane = std::max(g.cplane, j->plan.cplane);
             g.mplane = std::max(g.mplane, j->plan.mplane);
         }
-        begin.push_back(items);
         g.nitems = items;
         g.fixed_nx = g.jobs.front()->g.lnx;
         for (Job* j : g.jobs)
             if (j->g.lnx != g.fixed_nx) g.fixed_nx = 0;
-        g.mbatch = !g.fhm && jobs.size() > 1 && g.simple && !g.flat && g.nbuf == kMarchBatchNbuf;
+        g.mbatch = !g.fhm && shared && g.simple && !g.flat && g.nbuf == kMarchBatchNbuf;
         for (Job* j : g.jobs)
             if (!march_batch_job(j->g)) g.mbatch = false;
+    }
+    // a job-set change that fits the stable lanes: rewrite their tables,
+    // keep the graphs
+    if (stable_lanes && refresh_tables(ng)) {
+        ++refreshes_;
+        dirty_ = false;
+        return MG_OK;
+    }
+    ++rebuilds_;
+    drop_graphs();
+    free_groups();
+    groups_ = ng;
+    for (Group& g : groups_) {
+        if (g.generic) continue;
+        if (stable_lanes) {
+            // the largest tile this class has seen sizes the lane, so that
+            // later jobs fit it without a new capture
+            HighWater& h = hw_[{g.key, g.sub}];
+            h.block = std::max(h.block, g.block);
+            h.cplane = std::max(h.cplane, g.cplane);
+            h.mplane = std::max(h.mplane, g.mplane);
+            g.block = h.block;
+            g.cplane = h.cplane;
+            g.mplane = h.mplane;
+        }
         g.smem = g.fhm ? fh_smem(g.nbuf, g.cplane, g.mplane) : group_smem(g.nbuf, g.cplane, g.mplane, g.fp32 ? 4 : 8);
         if (g.smem > info.smem_optin) return fail(MG_EINVAL, "batch group needs %zu bytes of shared memory", g.smem);
         int occ = 1;
-        MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &occ, group_kernel(g), g.block, g.smem));
+        MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, group_kernel(g), g.block, g.smem));
         occ = std::max(occ, 1);
-        g.grid = std::min(items, info.sms * occ);
-        MG_CUDA(cudaMalloc(&g.d_item_begin, sizeof(int) * begin.size()));
-        MG_CUDA(cudaMalloc(&g.d_slot, sizeof(int) * slot.size()));
-        MG_CUDA(cudaMemcpy(g.d_item_begin, begin.data(), sizeof(int) * begin.size(), cudaMemcpyHostToDevice));
-        MG_CUDA(cudaMemcpy(g.d_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice));
+        // a stable lane keeps its grid whatever the item count: persistent CTAs
+        g.grid = stable_lanes ? info.sms * occ : std::min(g.nitems, info.sms * occ);
+        g.table_cap = stable_lanes ? std::max(capacity_, 1) : (int)g.jobs.size();
+        MG_CUDA(cudaMalloc(&g.d_item_begin, sizeof(int) * (g.table_cap + 1)));
+        MG_CUDA(cudaMalloc(&g.d_slot, sizeof(int) * g.table_cap));
+        if (stable_lanes) MG_CUDA(cudaMalloc(&g.d_counts, sizeof(int) * 2));
+        MG_TRY(write_tables(g));
     }
     // streams and events of the lanes (created here, never inside a capture)
     size_t lanes = 0;
@@ -1108,12 +1202,13 @@ int Engine::launch_lane(const Group& g, Job* generic_job, cudaStream_t st)
         }
         ch_step_generic_finish<<<1, 32, 0, st>>>(d_jobs_ + j->slot);
     } else {
-        StepArgs a;
+        StepArgs a{};
         a.jobs = d_jobs_;
         a.job_slot = g.d_slot;
         a.item_begin = g.d_item_begin;
         a.njobs = (int)g.jobs.size();
         a.nitems = g.nitems;
+        a.counts = g.d_counts;
         a.cplane = g.cplane;
         a.mplane = g.mplane;
         a.spin_limit = spin_limit();

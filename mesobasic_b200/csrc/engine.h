@@ -130,7 +130,8 @@ class Engine {
     int nitems_total() const;
     int nctas_total() const;
     int nlaunch_per_step() const;
-    long long rebuilds() const { return rebuilds_; }  // launch-set rebuilds so far
+    long long rebuilds() const { return rebuilds_; }  // launch-set rebuilds (graphs recaptured) so far
+    long long refreshes() const { return refreshes_; }  // job-set changes absorbed by rewriting lane tables
 
     int device = 0;
     // jobs share launches (batch, server): tile every job for equally full
@@ -146,6 +147,12 @@ class Engine {
     // whose job set changes often (the server) captures short graphs and
     // replays them back to back: each change costs one short capture.
     int graph_max_steps = 0;
+    // stable lanes (the server): each launch class keeps one lane whose job
+    // list, item offsets and counts live in device tables sized for the
+    // engine's capacity, with the block and shared memory of the largest
+    // tile the class has seen; a change of the job set that fits the lanes
+    // rewrites the tables and keeps the captured graphs
+    bool stable_lanes = false;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;  // created on first use (download_finished)
     DevInfo info;
@@ -156,6 +163,10 @@ class Engine {
         bool fp32 = false, flat = false, generic = false, simple = false, mass = false;
         bool mbatch = false;  // ch_march_batch_kernel: jobs of any march width
         bool fhm = false;     // fh_march_kernel: fused variable-mobility jobs
+        long long key = 0;    // launch class (precision, shape class, ring, width)
+        int sub = 0;          // index among the groups of one class
+        int* d_counts = nullptr;  // stable lanes: device [njobs, nitems]
+        int table_cap = 0;        // stable lanes: entries of d_slot (d_item_begin has one more)
         int nbuf = 4;
         std::vector<Job*> jobs;
         int nitems = 0, grid = 0, block = 0;
@@ -166,7 +177,14 @@ class Engine {
         int* d_slot = nullptr;
     };
     int rebuild();
+    bool refresh_tables(std::vector<Group>& ng);
+    int write_tables(const Group& g);
     StepKernel group_kernel(const Group& g) const;
+    struct HighWater {
+        int block = 0, cplane = 0, mplane = 0;
+    };
+    std::map<std::pair<long long, int>, HighWater> hw_;  // stable lanes: largest tile seen per class
+    long long refreshes_ = 0;
     void free_groups();
     int launch_lane(const Group& g, Job* generic_job, cudaStream_t st);
     int launch_steps(int k);

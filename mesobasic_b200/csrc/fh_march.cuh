@@ -59,6 +59,7 @@ __device__ __forceinline__ double lds1d(uint32_t a)
 template <int NBUF, bool FLAT>
 __global__ void __launch_bounds__(kFhBlock, 1) fh_march_kernel(StepArgs a)
 {
+    step_counts(a);
     using A = Arith<double>;
     constexpr int U = (NBUF % 3 == 0) ? NBUF : 3 * NBUF;
 

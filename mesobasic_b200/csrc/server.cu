@@ -255,6 +255,9 @@ int mg_server_create(int device, double hbm_budget_gb, int max_jobs_in_flight, i
     // admissions and retirements change the job set between ticks: short
     // graphs keep the recapture after each change cheap
     s->eng.graph_max_steps = mg::mg_env_int("MG_SERVER_GRAPH_STEPS", 10);
+    // job-set changes that fit the launch lanes rewrite device tables
+    // instead of recapturing the graphs
+    s->eng.stable_lanes = true;
     s->budget = hbm_budget_gb * 1e9;
     s->max_inflight = max_jobs_in_flight;
     s->steps_per_tick = steps_per_tick > 0 ? steps_per_tick : 100;
@@ -344,6 +347,7 @@ int mg_server_stats_get(mg_server_t* s, mg_server_stats* out)
     st.retire_s = s->retire_s;
     st.ticks = s->ticks;
     st.rebuilds = s->eng.rebuilds();
+    st.refreshes = s->eng.refreshes();
     st.queued = (long long)s->queue.size();
     if (!s->latencies_ms.empty()) {
         std::vector<double> v = s->latencies_ms;

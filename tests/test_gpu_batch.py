@@ -116,6 +116,36 @@ def test_server_results_identical_alone_and_mixed():
         srv.close()
 
 
+def test_server_absorbs_job_set_changes_without_recapture():
+    """A stream of 3-D FP32 jobs of march widths: after the first ticks set
+    up the launch lanes, admissions and retirements rewrite the lanes'
+    device tables instead of recapturing the step graph, and every result
+    is still bit-identical to its standalone run."""
+    rng = np.random.default_rng(5)
+    jobs = []
+    for j in range(14):
+        e = int(rng.choice([64, 96, 128]))
+        p = mb.make_params(e, e, e, 0.005, kappa=float(rng.uniform(0.5, 2.0)), precision="fp32")
+        jobs.append((p, mb.ic_generate((e, e, e), float(rng.uniform(-0.4, 0.4)), 0.05, False, 3000 + j),
+                     int(rng.integers(30, 90))))
+    srv = mb.Server(hbm_budget_gb=8.0, max_jobs=64, steps_per_tick=10)
+    try:
+        ids = []
+        for p, ic, n in jobs:
+            ids.append(srv.submit(p, ic, n))
+            time.sleep(0.003)
+        for (p, ic, n), jid in zip(jobs, ids):
+            got, st = srv.result(jid, p, timeout_us=120_000_000)
+            want, _ = alone(p, ic, n)
+            assert np.array_equal(got, want), jid
+        s = srv.stats()
+        assert s["completed"] == len(jobs) and s["failed"] == 0
+        assert s["refreshes"] > 0
+        assert s["rebuilds"] < s["ticks"]
+    finally:
+        srv.close()
+
+
 def test_server_admission_respects_budget():
     # budget fits two 128^3 FP64 jobs (2 x 2 x 16.8 MB) but not three
     p = mb.make_params(128, 128, 128, 0.005)
