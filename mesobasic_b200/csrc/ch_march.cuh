@@ -387,8 +387,13 @@ __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int loc
                     done = true;
                     break;
                 }
-                // planes <= i were last read above: their slots take the next planes
-                if (tid == producer && i + NBUF < nplanes) issue(i + NBUF, sI);
+                // planes <= i were last read above: slot i takes plane i+NBUF,
+                // and after the first plane slot 0 (plane 0, read only as a
+                // z-queue register in the prologue) takes plane NBUF
+                if (tid == producer) {
+                    if (i == 1 && NBUF < nplanes) issue(NBUF, 0);
+                    if (i + NBUF < nplanes) issue(i + NBUF, sI);
+                }
                 if constexpr (ORDER == 0) stage_b();
                 g += gstep;
             }
@@ -400,7 +405,9 @@ __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int loc
             // no copy lands after the CTA has exited; the job and the launch
             // are flagged
             if (tid == 0) {
-                const int nissued = min(nplanes, ifail - 1 + NBUF);
+                // planes issued before the barrier of plane ifail: NBUF at the start,
+                // then NBUF + 1 after plane 1 and one more after each later plane
+                const int nissued = min(nplanes, ifail >= 2 ? NBUF + ifail : NBUF);
                 for (int p = nw; p < nissued; ++p) {
                     const int s = p % NBUF;
                     mbar_wait_bounded(&head->bar[s], (ph >> s) & 1u, a.spin_limit);

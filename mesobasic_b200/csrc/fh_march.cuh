@@ -301,14 +301,22 @@ __global__ void __launch_bounds__(kFhBlock, 1) fh_march_kernel(StepArgs a)
                     done = true;
                     break;
                 }
-                if (tid == producer && i + NBUF < nplanes) issue(i + NBUF, sI);
+                // planes <= i were last read above: slot i takes plane i+NBUF,
+                // and after the first plane slot 0 (plane 0, read only as a
+                // z-queue register in the prologue) takes plane NBUF
+                if (tid == producer) {
+                    if (i == 1 && NBUF < nplanes) issue(NBUF, 0);
+                    if (i + NBUF < nplanes) issue(i + NBUF, sI);
+                }
                 g += gstep;
             }
             if (done) break;
         }
         if (ifail) {
             if (tid == 0) {
-                const int nissued = min(nplanes, ifail - 1 + NBUF);
+                // planes issued before the barrier of plane ifail: NBUF at the start,
+                // then NBUF + 1 after plane 1 and one more after each later plane
+                const int nissued = min(nplanes, ifail >= 2 ? NBUF + ifail : NBUF);
                 for (int p = nw; p < nissued; ++p) {
                     const int s = p % NBUF;
                     mbar_wait_bounded(&head->bar[s], (ph >> s) & 1u, a.spin_limit);
