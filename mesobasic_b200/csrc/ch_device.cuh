@@ -229,15 +229,45 @@ __device__ __forceinline__ int find_job(const int* item_begin, int njobs, int it
     return lo;
 }
 
-// The stored mass of one thread strip in 2^-32 units: its 8 values summed
-// in FP64 (exact conversions, fixed order), rounded once.  The same function
-// measures the field at upload and after every measured step.
+// The stored mass of one thread strip in 2^-32 units: each of its 8 values
+// rounded to the nearest multiple of 2^-32 (ties to even), the integers
+// added.  The rounding uses FP32 arithmetic and bit patterns only, no
+// conversion instructions: t = x + 1.5*2^14 rounds x to the 2^-9 grid
+// (hi = t - 1.5*2^14, exact), lo = x - hi is exact with |lo| <= 2^-10, and
+// y = lo*2^32 + 1.5*2^23 rounds lo*2^32 to an integer; on [2^14, 2^15) and
+// [2^23, 2^24) consecutive floats have consecutive bit patterns, so
+// bits(t) - bits(1.5*2^14) = hi/2^-9 and bits(y) - bits(1.5*2^23) = the
+// rounded lo*2^32.  Exact for |x| < 2^12.  The same function measures the
+// field at upload and after every measured step, so the measure does not
+// depend on the decomposition.
+__device__ __forceinline__ long long strip_mass(const Strip<float>& s)
+{
+    constexpr float kM1 = 24576.0f;     // 1.5 * 2^14
+    constexpr float kM2 = 12582912.0f;  // 1.5 * 2^23
+    const unsigned long long m1 = splat2(kM1), m2 = splat2(kM2), sc = splat2(kMassScale);
+    uint32_t ht = 0u, ly = 0u;  // sums of bit patterns, modulo 2^32
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const unsigned long long t = add2(s.p[k], m1);
+        const unsigned long long lo = sub2(s.p[k], sub2(t, m1));
+        const unsigned long long y = fma2(lo, sc, m2);
+        ht += (uint32_t)t + (uint32_t)(t >> 32);
+        ly += (uint32_t)y + (uint32_t)(y >> 32);
+    }
+    const int32_t h = (int32_t)(ht - 8u * __float_as_uint(kM1));  // in units of 2^-9
+    const int32_t l = (int32_t)(ly - 8u * __float_as_uint(kM2));  // in units of 2^-32
+    return (long long)h * 8388608LL + (long long)l;
+}
+
 __device__ __forceinline__ long long strip_mass(float o0, float o1, float o2, float o3, float o4, float o5, float o6,
                                                 float o7)
 {
-    const double x = ((double)o0 + (double)o2) + ((double)o4 + (double)o6);
-    const double y = ((double)o1 + (double)o3) + ((double)o5 + (double)o7);
-    return __double2ll_rn((x + y) * (double)kMassScale);
+    Strip<float> s;
+    s.p[0] = pk2(o0, o1);
+    s.p[1] = pk2(o2, o3);
+    s.p[2] = pk2(o4, o5);
+    s.p[3] = pk2(o6, o7);
+    return strip_mass(s);
 }
 
 // Does the nudge window [w0, w0 + |cnt|) (wrapping at nsites) reach the row

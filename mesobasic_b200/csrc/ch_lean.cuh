@@ -240,8 +240,7 @@ __global__ void __launch_bounds__(kMaxBlock, 1) ch_lean_kernel(StepArgs a)
 #pragma unroll
                             for (int k = 0; k < 4; ++k) out.p[k] = pk2(o[2 * k], o[2 * k + 1]);
                         }
-                        if (measure) macc += strip_mass(out.get(0), out.get(1), out.get(2), out.get(3), out.get(4), out.get(5),
-                                           out.get(6), out.get(7));
+                        if (measure) macc += strip_mass(out);
                     }
                     float* g = grow + zoff;
                     stg_v2(g, out.p[0], out.p[1]);

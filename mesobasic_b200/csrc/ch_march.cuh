@@ -376,8 +376,7 @@ __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int loc
                             }
                         }
                         if (measure)
-                            macc += strip_mass(out.get(0), out.get(1), out.get(2), out.get(3), out.get(4), out.get(5),
-                                               out.get(6), out.get(7));
+                            macc += strip_mass(out);
                     }
                     IO::stg(g, NXC / 2, out);
                 };

@@ -46,10 +46,9 @@ enum DeviceError : int {
 constexpr float kNudge = 1.1920928955078125e-7f;  // 2^-23
 
 // The stored mass is measured the same way by the step kernel and at upload,
-// independent of the decomposition: each thread strip's 8 values are summed
-// in FP64 in one fixed order (strip_mass), the sum is rounded to a multiple
-// of 2^-32 and the integers are added (integer addition does not depend on
-// order).  A strip is the 8 sites x = 4t..4t+3 and nx/2 + 4t..4t+3 of a row.
+// independent of the decomposition: each value is rounded to the nearest
+// multiple of 2^-32 (strip_mass, exact for |c| < 2^12) and the integers are
+// added (integer addition does not depend on order).
 constexpr float kMassScale = 4294967296.0f;  // 2^32
 
 // Which per-site chemical potential and mobility a variable-mobility job
