@@ -482,7 +482,7 @@ __device__ __noinline__ uint32_t march_item_call(StepArgs a, JobDev* J, int loca
                                                  uint32_t mbase, uint32_t bar0, uint32_t ph)
 {
     MarchCta cta{head, cbase, mbase, bar0, ph};
-    const bool ok = march_item<T, NXC, NBUF, MASS, 1>(a, J, local, cta);
+    const bool ok = march_item<T, NXC, NBUF, MASS, 0>(a, J, local, cta);
     return cta.ph | (ok ? 0u : 0x80000000u);
 }
 
@@ -520,6 +520,39 @@ __global__ void __launch_bounds__(kMaxBlock, 1) ch_march_batch_kernel(StepArgs a
         }
 #undef MG_MARCH_CASE
         if (ph & 0x80000000u) return;
+    }
+}
+
+// The same with every width's item body inlined into the kernel.
+template <typename T, int NBUF, bool MASS>
+__global__ void __launch_bounds__(kMaxBlock, 1) ch_march_batch_inline_kernel(StepArgs a)
+{
+    step_counts(a);
+    MarchCta cta = march_setup<NBUF>(a, sizeof(T));
+    for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
+        const int j = find_job(a.item_begin, a.njobs, item);
+        JobDev* J = a.jobs + __ldg(a.job_slot + j);
+        const int local = item - __ldg(a.item_begin + j);
+        bool ok;
+        if constexpr (sizeof(T) == 4) {
+            switch (J->nx) {
+            case 64: ok = march_item<T, 64, NBUF, MASS, 0>(a, J, local, cta); break;
+            case 96: ok = march_item<T, 96, NBUF, MASS, 0>(a, J, local, cta); break;
+            case 128: ok = march_item<T, 128, NBUF, MASS, 0>(a, J, local, cta); break;
+            case 160: ok = march_item<T, 160, NBUF, MASS, 0>(a, J, local, cta); break;
+            case 192: ok = march_item<T, 192, NBUF, MASS, 0>(a, J, local, cta); break;
+            case 224: ok = march_item<T, 224, NBUF, MASS, 0>(a, J, local, cta); break;
+            default: ok = march_item<T, 256, NBUF, MASS, 0>(a, J, local, cta); break;
+            }
+        } else {
+            switch (J->nx) {
+            case 64: ok = march_item<T, 64, NBUF, MASS, 0>(a, J, local, cta); break;
+            case 128: ok = march_item<T, 128, NBUF, MASS, 0>(a, J, local, cta); break;
+            case 192: ok = march_item<T, 192, NBUF, MASS, 0>(a, J, local, cta); break;
+            default: ok = march_item<T, 256, NBUF, MASS, 0>(a, J, local, cta); break;
+            }
+        }
+        if (!ok) return;
     }
 }
 

@@ -20,6 +20,8 @@
 
 namespace mg {
 
+static bool march_enabled();
+
 // ------------------------------------------------------------------ errors
 static thread_local std::string t_err;
 
@@ -181,7 +183,11 @@ static bool fixed_width(int nx, int nbuf)
 
 bool fixed_width_kernel(const Geometry& g, int nbuf)
 {
-    return geometry_simple(g) && !g.flat && fixed_width(g.lnx, nbuf);
+    if (!geometry_simple(g) || g.flat) return false;
+    if (fixed_width(g.lnx, nbuf)) return true;
+    // a march variant (launch bound kMaxBlock) for this width and ring depth
+    return march_enabled() &&
+           (g.es == 4 ? march_kernel_f32(g.lnx, nbuf, false, 0) : march_kernel_f64(g.lnx, nbuf, 0)) != nullptr;
 }
 
 int plan_tiling(const Geometry& g, const mg_tiling& t, const DevInfo& d, TilePlan* out)
@@ -297,9 +303,10 @@ static mg_tiling fh_default_tiling(const Geometry& g, const DevInfo& d)
             clear_error();
         }
     const int ntile = g.flat ? 1 : (g.lny + ty - 1) / ty;
-    int nchunk = std::max(1, d.sms / ntile);
+    int nchunk = std::max(1, (3 * d.sms + ntile - 1) / ntile);  // about three waves of items
     nchunk = std::min(nchunk, std::max(1, g.lnz / 8));
-    if (nchunk > 1 && (nchunk & 1)) nchunk -= 1;
+    if (nchunk > 1 && (nchunk & 1)) nchunk += 1;
+    nchunk = std::min(nchunk, g.lnz);
     return mg_tiling{ty, nchunk, 3, 0};
 }
 
@@ -370,7 +377,17 @@ static int march_order()
 {
     static const int v = [] {
         const char* e = std::getenv("MG_MARCH_ORDER");
-        return e && e[0] == '0' ? 0 : 1;
+        return e && e[0] == '1' ? 1 : 0;
+    }();
+    return v;
+}
+// one launch for every width of a shared engine: 0 off (a launch per
+// width class), 1 per-width calls, 2 per-width bodies inlined
+static int march_batch_mode()
+{
+    static const int v = [] {
+        const char* e = std::getenv("MG_MARCH_BATCH");
+        return e ? std::atoi(e) : 1;
     }();
     return v;
 }
@@ -407,7 +424,8 @@ bool nbuf_ok(int nbuf) { return nbuf == 3 || nbuf == 4 || nbuf == 6 || nbuf == 8
 
 bool march_batch_job(const Geometry& g)
 {
-    return march_enabled() && geometry_simple(g) && !g.flat && tma_shape_ok(g) && march_batch_width(g.es, g.lnx);
+    return march_enabled() && march_batch_mode() != 0 && geometry_simple(g) && !g.flat && tma_shape_ok(g) &&
+           march_batch_width(g.es, g.lnx);
 }
 
 int prepare_kernels(const DevInfo& d)
@@ -431,11 +449,13 @@ int prepare_kernels(const DevInfo& d)
     MG_CUDA(cudaFuncSetAttribute(fh_march_kernel<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));
     for (int nb : {3, 6})
         for (int ms = 0; ms < 2; ++ms) {
-            MG_CUDA(cudaFuncSetAttribute(march_batch_kernel_f32(nb, ms), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)d.smem_optin));
-            if (!ms)
-                MG_CUDA(cudaFuncSetAttribute(march_batch_kernel_f64(nb), cudaFuncAttributeMaxDynamicSharedMemorySize,
+            for (int inl = 0; inl < 2; ++inl) {
+                MG_CUDA(cudaFuncSetAttribute(march_batch_kernel_f32(nb, ms, inl), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)d.smem_optin));
+                if (!ms)
+                    MG_CUDA(cudaFuncSetAttribute(march_batch_kernel_f64(nb, inl),
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));
+            }
         }
     done = true;
     return MG_OK;
@@ -935,7 +955,8 @@ StepKernel Engine::group_kernel(const Group& g) const
 {
     if (g.fhm) return g.flat ? fh_march_kernel<3, true> : fh_march_kernel<3, false>;
     if (g.mbatch) {
-        StepKernel k = g.fp32 ? march_batch_kernel_f32(g.nbuf, g.mass) : march_batch_kernel_f64(g.nbuf);
+        const bool inl = march_batch_mode() == 2;
+        StepKernel k = g.fp32 ? march_batch_kernel_f32(g.nbuf, g.mass, inl) : march_batch_kernel_f64(g.nbuf, inl);
         if (k) return k;
     }
     return step_kernel(g.fp32, g.flat, g.nbuf, g.simple, g.block, g.mass, g.fixed_nx);

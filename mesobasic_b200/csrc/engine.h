@@ -229,8 +229,8 @@ bool nbuf_ok(int nbuf);
 StepKernel march_kernel_f32(int nx, int nbuf, bool mass, int order);
 StepKernel march_kernel_f64(int nx, int nbuf, int order);
 // one launch for jobs of every march width (ring depths 3 and 6)
-StepKernel march_batch_kernel_f32(int nbuf, bool mass);
-StepKernel march_batch_kernel_f64(int nbuf);
+StepKernel march_batch_kernel_f32(int nbuf, bool mass, bool inlined = false);
+StepKernel march_batch_kernel_f64(int nbuf, bool inlined = false);
 bool march_batch_job(const Geometry& g);  // a job the batch kernel takes
 // ring depth of march jobs that share launches (batch, server)
 constexpr int kMarchBatchNbuf = 6;

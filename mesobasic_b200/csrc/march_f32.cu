@@ -49,11 +49,15 @@ StepKernel march_kernel_f32(int nx, int nbuf, bool mass, int order)
     return mass ? march_f32_width<true>(nx, nbuf, order) : march_f32_width<false>(nx, nbuf, order);
 }
 
-StepKernel march_batch_kernel_f32(int nbuf, bool mass)
+StepKernel march_batch_kernel_f32(int nbuf, bool mass, bool inlined)
 {
     switch (nbuf) {
-    case 3: return mass ? ch_march_batch_kernel<float, 3, true> : ch_march_batch_kernel<float, 3, false>;
-    case 6: return mass ? ch_march_batch_kernel<float, 6, true> : ch_march_batch_kernel<float, 6, false>;
+    case 3:
+        if (inlined) return mass ? ch_march_batch_inline_kernel<float, 3, true> : ch_march_batch_inline_kernel<float, 3, false>;
+        return mass ? ch_march_batch_kernel<float, 3, true> : ch_march_batch_kernel<float, 3, false>;
+    case 6:
+        if (inlined) return mass ? ch_march_batch_inline_kernel<float, 6, true> : ch_march_batch_inline_kernel<float, 6, false>;
+        return mass ? ch_march_batch_kernel<float, 6, true> : ch_march_batch_kernel<float, 6, false>;
     default: return nullptr;
     }
 }

@@ -28,11 +28,11 @@ static StepKernel march_f64_nbuf(int nbuf, int order)
     }
 }
 
-StepKernel march_batch_kernel_f64(int nbuf)
+StepKernel march_batch_kernel_f64(int nbuf, bool inlined)
 {
     switch (nbuf) {
-    case 3: return ch_march_batch_kernel<double, 3, false>;
-    case 6: return ch_march_batch_kernel<double, 6, false>;
+    case 3: return inlined ? ch_march_batch_inline_kernel<double, 3, false> : ch_march_batch_kernel<double, 3, false>;
+    case 6: return inlined ? ch_march_batch_inline_kernel<double, 6, false> : ch_march_batch_kernel<double, 6, false>;
     default: return nullptr;
     }
 }
