@@ -627,6 +627,9 @@ __device__ __forceinline__ size_t fh_at(int x, int y, int z, const JobDev& J)
     return ((size_t)z * J.ny + y) * J.nx + x;
 }
 
+// Pass 1: mu and the reciprocal mobility 1/mob of every site (F.mu, F.mob).
+// A thread keeps one x for all its sites (the grid's stride is a multiple
+// of nx), so the per-x constants of the step (fh_column) are formed once.
 __global__ void fh_mu_mob_kernel(JobDev* job)
 {
     using A = Arith<double>;
@@ -634,39 +637,39 @@ __global__ void fh_mu_mob_kernel(JobDev* job)
     const FhDev& F = *J.fh;
     const int nx = J.nx, ny = J.ny, nz = J.nz;
     const size_t n = (size_t)nx * ny * nz;
-    const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (J.step >= J.target || s >= n) return;
+    if (J.step >= J.target) return;
     const double* __restrict__ c = static_cast<const double*>(J.buf[J.step & 1]);
     // the step being taken (PFApp passes it as current_step)
     const double cs = (double)(J.step + 1);
-    const int x = (int)(s % nx), y = (int)((s / nx) % ny), z = (int)(s / ((size_t)nx * ny));
     const bool pX = J.flags & JF_PER_X, pY = J.flags & JF_PER_Y, pZ = J.flags & JF_PER_Z;
-    const double cc = c[s];
-    const double xp = c[fh_at(wrap_or_clamp(x + 1, nx, pX), y, z, J)], xm = c[fh_at(wrap_or_clamp(x - 1, nx, pX), y, z, J)];
-    const double zp = c[fh_at(x, y, wrap_or_clamp(z + 1, nz, pZ), J)], zm = c[fh_at(x, y, wrap_or_clamp(z - 1, nz, pZ), J)];
-    double lapc;
-    if (J.flags & JF_FLAT) {
-        lapc = A::add(axis_term(xp, xm, cc, J.cx, J.flags & JF_DIV_X), axis_term(zp, zm, cc, J.cz, J.flags & JF_DIV_Z));
-    } else {
-        const double yp = c[fh_at(x, wrap_or_clamp(y + 1, ny, pY), z, J)], ym = c[fh_at(x, wrap_or_clamp(y - 1, ny, pY), z, J)];
-        lapc = A::add(A::add(axis_term(xp, xm, cc, J.cx, J.flags & JF_DIV_X), axis_term(yp, ym, cc, J.cy, J.flags & JF_DIV_Y)),
-                      axis_term(zp, zm, cc, J.cz, J.flags & JF_DIV_Z));
+    const size_t first = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;  // a multiple of nx (the host's launch)
+    const int x = (int)(first % nx);
+    const FhCol col = fh_column(F, x, cs, J.dtM_dt);
+    for (size_t s = first; s < n; s += stride) {
+        const int y = (int)((s / nx) % ny), z = (int)(s / ((size_t)nx * ny));
+        const double cc = c[s];
+        const double xp = c[fh_at(wrap_or_clamp(x + 1, nx, pX), y, z, J)], xm = c[fh_at(wrap_or_clamp(x - 1, nx, pX), y, z, J)];
+        const double zp = c[fh_at(x, y, wrap_or_clamp(z + 1, nz, pZ), J)], zm = c[fh_at(x, y, wrap_or_clamp(z - 1, nz, pZ), J)];
+        double lapc;
+        if (J.flags & JF_FLAT) {
+            lapc = A::add(axis_term(xp, xm, cc, J.cx, J.flags & JF_DIV_X), axis_term(zp, zm, cc, J.cz, J.flags & JF_DIV_Z));
+        } else {
+            const double yp = c[fh_at(x, wrap_or_clamp(y + 1, ny, pY), z, J)], ym = c[fh_at(x, wrap_or_clamp(y - 1, ny, pY), z, J)];
+            lapc = A::add(A::add(axis_term(xp, xm, cc, J.cx, J.flags & JF_DIV_X), axis_term(yp, ym, cc, J.cy, J.flags & JF_DIV_Y)),
+                          axis_term(zp, zm, cc, J.cz, J.flags & JF_DIV_Z));
+        }
+        double mu, mob;
+        fh_site_col(F, col, cc, lapc, J.kap, &mu, &mob);
+        F.mu[s] = mu;
+        F.mob[s] = A::div(1.0, mob);  // the reciprocal every face of the site uses
     }
-    fh_site(F, cc, lapc, J.kap, x, cs, J.dtM_dt, F.mu + s, F.mob + s);
 }
 
-// (a[-]*b1 + a[+]*b2 - (b1+b2)*a) / d^2 with b1, b2 the harmonic means of
-// the mobilities toward each neighbour
-__device__ __forceinline__ double fh_axis(double am, double ap, double a0, double bm, double bp, double bo, double coef,
-                                          bool divide)
-{
-    using A = Arith<double>;
-    const double b1 = A::div(2.0, A::add(A::div(1.0, bm), A::div(1.0, bo)));
-    const double b2 = A::div(2.0, A::add(A::div(1.0, bp), A::div(1.0, bo)));
-    const double num = A::sub(A::add(A::mul(am, b1), A::mul(ap, b2)), A::mul(A::add(b1, b2), a0));
-    return divide ? A::div(num, coef) : A::mul(num, coef);
-}
-
+// Pass 2: c += dt * div(mob grad mu) (SfieldFD::Laplacian(const SfieldFD&),
+// SfieldFD.cpp:333-355) from mu and the reciprocal mobilities of pass 1:
+// each face's harmonic mean 2/(1/mob_a + 1/mob_b) from the two stored
+// reciprocals -- the reference's operands in its order, so the same value.
 __global__ void fh_update_kernel(JobDev* job)
 {
     using A = Arith<double>;
@@ -680,20 +683,20 @@ __global__ void fh_update_kernel(JobDev* job)
     const double* __restrict__ c = static_cast<const double*>(J.buf[par]);
     double* __restrict__ out = static_cast<double*>(J.buf[par ^ 1]);
     const double* __restrict__ mu = F.mu;
-    const double* __restrict__ mob = F.mob;
+    const double* __restrict__ rmob = F.mob;
     const int x = (int)(s % nx), y = (int)((s / nx) % ny), z = (int)(s / ((size_t)nx * ny));
     const bool pX = J.flags & JF_PER_X, pY = J.flags & JF_PER_Y, pZ = J.flags & JF_PER_Z;
-    const double a0 = mu[s], bo = mob[s];
+    const double a0 = mu[s], ro = rmob[s];
     const size_t ixm = fh_at(wrap_or_clamp(x - 1, nx, pX), y, z, J), ixp = fh_at(wrap_or_clamp(x + 1, nx, pX), y, z, J);
     const size_t izm = fh_at(x, y, wrap_or_clamp(z - 1, nz, pZ), J), izp = fh_at(x, y, wrap_or_clamp(z + 1, nz, pZ), J);
-    const double lx = fh_axis(mu[ixm], mu[ixp], a0, mob[ixm], mob[ixp], bo, J.cx, J.flags & JF_DIV_X);
-    const double lz = fh_axis(mu[izm], mu[izp], a0, mob[izm], mob[izp], bo, J.cz, J.flags & JF_DIV_Z);
+    const double lx = fh_axis_r(mu[ixm], mu[ixp], a0, rmob[ixm], rmob[ixp], ro, J.cx, J.flags & JF_DIV_X);
+    const double lz = fh_axis_r(mu[izm], mu[izp], a0, rmob[izm], rmob[izp], ro, J.cz, J.flags & JF_DIV_Z);
     double lap;
     if (J.flags & JF_FLAT) {
         lap = A::add(lx, lz);
     } else {
         const size_t iym = fh_at(x, wrap_or_clamp(y - 1, ny, pY), z, J), iyp = fh_at(x, wrap_or_clamp(y + 1, ny, pY), z, J);
-        const double ly = fh_axis(mu[iym], mu[iyp], a0, mob[iym], mob[iyp], bo, J.cy, J.flags & JF_DIV_Y);
+        const double ly = fh_axis_r(mu[iym], mu[iyp], a0, rmob[iym], rmob[iyp], ro, J.cy, J.flags & JF_DIV_Y);
         lap = A::add(A::add(lx, ly), lz);
     }
     out[s] = A::add(c[s], A::mul(J.dtM_dt, lap));  // c += dt * lap (TIPSphil.cpp:194)

@@ -16,6 +16,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <numeric>
 #include <thread>
 
 namespace mg {
@@ -797,7 +798,7 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const Fh
     if (fh) {
         // the fused variable-mobility kernel where the shape allows, else the
         // per-site path (path 1)
-        j->tiling = fh_default_tiling(j->g, info);
+        j->tiling = mg_env_int("MG_FH_FUSED", 1) == 1 ? fh_default_tiling(j->g, info) : mg_tiling{1, 1, 4, 1};
         MG_TRY(plan_fh_tiling(j->g, j->tiling, info, &j->plan));
     } else {
         j->tiling = batch_tiling ? batch_tiling_for(j->g, info, device, batch_threads, batch_planes)
@@ -1213,8 +1214,12 @@ int Engine::launch_lane(const Group& g, Job* generic_job, cudaStream_t st)
     if (g.generic) {
         Job* j = generic_job;
         const unsigned blocks = (unsigned)((j->g.n + 255) / 256);
-        if (j->d_fh) {  // variable mobility: mu and mobility, then the update
-            fh_mu_mob_kernel<<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
+        if (j->d_fh) {  // variable mobility: mu and 1/mob, then the update
+            // pass 1's grid stride is a multiple of nx, so each thread keeps one x
+            const long long l = std::lcm((long long)j->g.lnx, 256LL);
+            long long q = std::max(1LL, 8LL * info.sms * 256 / l);
+            q = std::min(q, std::max(1LL, (long long)((j->g.n + l - 1) / l)));
+            fh_mu_mob_kernel<<<(unsigned)(l * q / 256), 256, 0, st>>>(d_jobs_ + j->slot);
             fh_update_kernel<<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
         } else if (g.fp32) {
             ch_step_generic_kernel<float><<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
