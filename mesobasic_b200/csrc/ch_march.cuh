@@ -11,14 +11,9 @@
 //    compile-time constants; each item starts its planes at ring slot 0,
 //    and the mbarrier parity of a slot is one bit of a mask that flips on
 //    every completed wait;
-//  - a plane is "wait for c(i+1); mu on plane i; c_new on plane i-1;
-//    barrier" (ORDER 1): stage B of plane i-1 reads the mu rows of plane
-//    i-1, which the previous barrier published, and mu(i) of its own sites
-//    from registers, so stages A and B share one straight stretch of code
-//    with no barrier between them and the compiler interleaves the two.
-//    The barrier then guards the mu slot the next plane overwrites and the
-//    c slot the producer refills.  ORDER 0 keeps the barrier between the
-//    stages, as ch_step_kernel has it.
+//  - a plane is "wait for c(i+1); mu on plane i; barrier; refill; c_new on
+//    plane i-1".  (Running stage B before the barrier, so that both stages
+//    share one stretch, measured 1-7 % slower.)
 //  - x-neighbours: FP32 rows whose threads form a power-of-two segment of
 //    a warp take them from warp shuffles; other rows (FP64, FP32 widths 96,
 //    160, 192, 224) from the row in shared memory.
@@ -161,7 +156,7 @@ __device__ __forceinline__ MarchCta march_setup(const StepArgs& a, uint32_t es)
 // One work item (y-tile x z-chunk) of job J, slot `local` among its items.
 // Returns false when a bounded wait ran out (the CTA must exit; the job and
 // the launch are flagged and the copies in flight drained).
-template <typename T, int NXC, int NBUF, bool MASS, int ORDER>
+template <typename T, int NXC, int NBUF, bool MASS>
 __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int local, MarchCta& cta)
 {
     constexpr int W = Strip<T>::W, HW = W / 2;
@@ -380,7 +375,6 @@ __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int loc
                     }
                     IO::stg(g, NXC / 2, out);
                 };
-                if constexpr (ORDER == 1) stage_b();
                 if (__syncthreads_or(failed)) {
                     ifail = i;
                     done = true;
@@ -393,7 +387,7 @@ __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int loc
                     if (i == 1 && NBUF < nplanes) issue(NBUF, 0);
                     if (i + NBUF < nplanes) issue(i + NBUF, sI);
                 }
-                if constexpr (ORDER == 0) stage_b();
+                stage_b();
                 g += gstep;
             }
             if (done) break;
@@ -461,7 +455,7 @@ __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int loc
 }
 
 // One job class: every job of the launch has row width NXC.
-template <typename T, int NXC, int NBUF, bool MASS, int ORDER>
+template <typename T, int NXC, int NBUF, bool MASS>
 __global__ void __launch_bounds__(kMaxBlock, 1) ch_march_kernel(StepArgs a)
 {
     step_counts(a);
@@ -470,97 +464,8 @@ __global__ void __launch_bounds__(kMaxBlock, 1) ch_march_kernel(StepArgs a)
         const int j = find_job(a.item_begin, a.njobs, item);
         JobDev* J = a.jobs + __ldg(a.job_slot + j);
         const int local = item - __ldg(a.item_begin + j);
-        if (!march_item<T, NXC, NBUF, MASS, ORDER>(a, J, local, cta)) return;
+        if (!march_item<T, NXC, NBUF, MASS>(a, J, local, cta)) return;
     }
-}
-
-// One item of a width-NXC job as a call of its own: each width is compiled
-// with its own register allocation when one kernel dispatches to several.
-// Returns the ring parity mask, with bit 31 set when the CTA must exit.
-template <typename T, int NXC, int NBUF, bool MASS>
-__device__ __noinline__ uint32_t march_item_call(StepArgs a, JobDev* J, int local, SmemHead* head, uint32_t cbase,
-                                                 uint32_t mbase, uint32_t bar0, uint32_t ph)
-{
-    MarchCta cta{head, cbase, mbase, bar0, ph};
-    const bool ok = march_item<T, NXC, NBUF, MASS, 0>(a, J, local, cta);
-    return cta.ph | (ok ? 0u : 0x80000000u);
-}
-
-// Jobs of every row width the march kernels take, in one persistent launch:
-// each item is dispatched to the variant of its job's width (uniform per
-// CTA).  Ring slots and parities carry over between items of any width.
-template <typename T, int NBUF, bool MASS>
-__global__ void __launch_bounds__(kMaxBlock, 1) ch_march_batch_kernel(StepArgs a)
-{
-    step_counts(a);
-    MarchCta cta = march_setup<NBUF>(a, sizeof(T));
-    uint32_t ph = cta.ph;
-    for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
-        const int j = find_job(a.item_begin, a.njobs, item);
-        JobDev* J = a.jobs + __ldg(a.job_slot + j);
-        const int local = item - __ldg(a.item_begin + j);
-#define MG_MARCH_CASE(W) ph = march_item_call<T, W, NBUF, MASS>(a, J, local, cta.head, cta.cbase, cta.mbase, cta.bar0, ph)
-        if constexpr (sizeof(T) == 4) {
-            switch (J->nx) {
-            case 64: MG_MARCH_CASE(64); break;
-            case 96: MG_MARCH_CASE(96); break;
-            case 128: MG_MARCH_CASE(128); break;
-            case 160: MG_MARCH_CASE(160); break;
-            case 192: MG_MARCH_CASE(192); break;
-            case 224: MG_MARCH_CASE(224); break;
-            default: MG_MARCH_CASE(256); break;
-            }
-        } else {
-            switch (J->nx) {
-            case 64: MG_MARCH_CASE(64); break;
-            case 128: MG_MARCH_CASE(128); break;
-            case 192: MG_MARCH_CASE(192); break;
-            default: MG_MARCH_CASE(256); break;
-            }
-        }
-#undef MG_MARCH_CASE
-        if (ph & 0x80000000u) return;
-    }
-}
-
-// The same with every width's item body inlined into the kernel.
-template <typename T, int NBUF, bool MASS>
-__global__ void __launch_bounds__(kMaxBlock, 1) ch_march_batch_inline_kernel(StepArgs a)
-{
-    step_counts(a);
-    MarchCta cta = march_setup<NBUF>(a, sizeof(T));
-    for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
-        const int j = find_job(a.item_begin, a.njobs, item);
-        JobDev* J = a.jobs + __ldg(a.job_slot + j);
-        const int local = item - __ldg(a.item_begin + j);
-        bool ok;
-        if constexpr (sizeof(T) == 4) {
-            switch (J->nx) {
-            case 64: ok = march_item<T, 64, NBUF, MASS, 0>(a, J, local, cta); break;
-            case 96: ok = march_item<T, 96, NBUF, MASS, 0>(a, J, local, cta); break;
-            case 128: ok = march_item<T, 128, NBUF, MASS, 0>(a, J, local, cta); break;
-            case 160: ok = march_item<T, 160, NBUF, MASS, 0>(a, J, local, cta); break;
-            case 192: ok = march_item<T, 192, NBUF, MASS, 0>(a, J, local, cta); break;
-            case 224: ok = march_item<T, 224, NBUF, MASS, 0>(a, J, local, cta); break;
-            default: ok = march_item<T, 256, NBUF, MASS, 0>(a, J, local, cta); break;
-            }
-        } else {
-            switch (J->nx) {
-            case 64: ok = march_item<T, 64, NBUF, MASS, 0>(a, J, local, cta); break;
-            case 128: ok = march_item<T, 128, NBUF, MASS, 0>(a, J, local, cta); break;
-            case 192: ok = march_item<T, 192, NBUF, MASS, 0>(a, J, local, cta); break;
-            default: ok = march_item<T, 256, NBUF, MASS, 0>(a, J, local, cta); break;
-            }
-        }
-        if (!ok) return;
-    }
-}
-
-// row widths the batch kernel dispatches (the host groups only these)
-__host__ __device__ constexpr bool march_batch_width(int es, int nx)
-{
-    return es == 4 ? (nx == 64 || nx == 96 || nx == 128 || nx == 160 || nx == 192 || nx == 224 || nx == 256)
-                   : (nx == 64 || nx == 128 || nx == 192 || nx == 256);
 }
 
 }  // namespace mg

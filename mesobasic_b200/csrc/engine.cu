@@ -188,7 +188,7 @@ bool fixed_width_kernel(const Geometry& g, int nbuf)
     if (fixed_width(g.lnx, nbuf)) return true;
     // a march variant (launch bound kMaxBlock) for this width and ring depth
     return march_enabled() &&
-           (g.es == 4 ? march_kernel_f32(g.lnx, nbuf, false, 0) : march_kernel_f64(g.lnx, nbuf, 0)) != nullptr;
+           (g.es == 4 ? march_kernel_f32(g.lnx, nbuf, false) : march_kernel_f64(g.lnx, nbuf)) != nullptr;
 }
 
 int plan_tiling(const Geometry& g, const mg_tiling& t, const DevInfo& d, TilePlan* out)
@@ -372,26 +372,7 @@ static StepKernel pick_shape(bool flat, bool simple, int nbuf, int block)
     return simple ? pick_maxt<T, false, true, MASS>(nbuf, block) : pick_maxt<T, false, false, MASS>(nbuf, block);
 }
 
-// stage order of the march kernels (MG_MARCH_ORDER=0: barrier between the
-// stages, as ch_step_kernel); MG_MARCH=0 selects the earlier kernels
-static int march_order()
-{
-    static const int v = [] {
-        const char* e = std::getenv("MG_MARCH_ORDER");
-        return e && e[0] == '1' ? 1 : 0;
-    }();
-    return v;
-}
-// one launch for every width of a shared engine: 0 off (a launch per
-// width class), 1 per-width calls, 2 per-width bodies inlined
-static int march_batch_mode()
-{
-    static const int v = [] {
-        const char* e = std::getenv("MG_MARCH_BATCH");
-        return e ? std::atoi(e) : 1;
-    }();
-    return v;
-}
+// MG_MARCH=0 selects the earlier kernels (ch_step_kernel, ch_lean_kernel)
 static bool march_enabled()
 {
     static const bool v = [] {
@@ -404,7 +385,7 @@ static bool march_enabled()
 StepKernel step_kernel(bool fp32, bool flat, int nbuf, bool simple, int block, bool mass, int nx)
 {
     if (simple && !flat && nx > 0 && march_enabled()) {
-        StepKernel k = fp32 ? march_kernel_f32(nx, nbuf, mass, march_order()) : march_kernel_f64(nx, nbuf, march_order());
+        StepKernel k = fp32 ? march_kernel_f32(nx, nbuf, mass) : march_kernel_f64(nx, nbuf);
         if (k) return k;
     }
     if (fp32 && simple && !flat && nx > 0) {
@@ -425,8 +406,8 @@ bool nbuf_ok(int nbuf) { return nbuf == 3 || nbuf == 4 || nbuf == 6 || nbuf == 8
 
 bool march_batch_job(const Geometry& g)
 {
-    return march_enabled() && march_batch_mode() != 0 && geometry_simple(g) && !g.flat && tma_shape_ok(g) &&
-           march_batch_width(g.es, g.lnx);
+    if (!march_enabled() || !geometry_simple(g) || g.flat || !tma_shape_ok(g)) return false;
+    return (g.es == 4 ? march_kernel_f32(g.lnx, kMarchBatchNbuf, false) : march_kernel_f64(g.lnx, kMarchBatchNbuf)) != nullptr;
 }
 
 int prepare_kernels(const DevInfo& d)
@@ -448,16 +429,6 @@ int prepare_kernels(const DevInfo& d)
                                                              (int)d.smem_optin));
     MG_CUDA(cudaFuncSetAttribute(fh_march_kernel<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));
     MG_CUDA(cudaFuncSetAttribute(fh_march_kernel<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));
-    for (int nb : {3, 6})
-        for (int ms = 0; ms < 2; ++ms) {
-            for (int inl = 0; inl < 2; ++inl) {
-                MG_CUDA(cudaFuncSetAttribute(march_batch_kernel_f32(nb, ms, inl), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)d.smem_optin));
-                if (!ms)
-                    MG_CUDA(cudaFuncSetAttribute(march_batch_kernel_f64(nb, inl),
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));
-            }
-        }
     done = true;
     return MG_OK;
 }
@@ -955,11 +926,6 @@ void Engine::free_graveyard()
 StepKernel Engine::group_kernel(const Group& g) const
 {
     if (g.fhm) return g.flat ? fh_march_kernel<3, true> : fh_march_kernel<3, false>;
-    if (g.mbatch) {
-        const bool inl = march_batch_mode() == 2;
-        StepKernel k = g.fp32 ? march_batch_kernel_f32(g.nbuf, g.mass, inl) : march_batch_kernel_f64(g.nbuf, inl);
-        if (k) return k;
-    }
     return step_kernel(g.fp32, g.flat, g.nbuf, g.simple, g.block, g.mass, g.fixed_nx);
 }
 
@@ -1086,9 +1052,7 @@ int Engine::rebuild()
         }
         const bool simple = geometry_simple(j->g);
         const bool mass = j->p.mass_correct && j->g.es == 4;
-        // several jobs of march widths: one launch for all widths (-1)
-        const bool mb = shared && march_batch_job(j->g) && j->tiling.nbuf == kMarchBatchNbuf;
-        const int fixed = mb ? -1 : (fixed_width_kernel(j->g, j->tiling.nbuf) ? j->g.lnx : 0);
+        const int fixed = fixed_width_kernel(j->g, j->tiling.nbuf) ? j->g.lnx : 0;
         const long long key = (long long)((j->g.es == 4 ? 1 : 0) | (j->g.flat ? 2 : 0) | (simple ? 4 : 0) |
                                           (mass ? 8 : 0) | (j->tiling.nbuf << 4)) |
                               ((long long)fixed << 12);
@@ -1129,9 +1093,6 @@ int Engine::rebuild()
         g.fixed_nx = g.jobs.front()->g.lnx;
         for (Job* j : g.jobs)
             if (j->g.lnx != g.fixed_nx) g.fixed_nx = 0;
-        g.mbatch = !g.fhm && shared && g.simple && !g.flat && g.nbuf == kMarchBatchNbuf;
-        for (Job* j : g.jobs)
-            if (!march_batch_job(j->g)) g.mbatch = false;
     }
     // a job-set change that fits the stable lanes: rewrite their tables,
     // keep the graphs

@@ -161,7 +161,6 @@ class Engine {
    private:
     struct Group {
         bool fp32 = false, flat = false, generic = false, simple = false, mass = false;
-        bool mbatch = false;  // ch_march_batch_kernel: jobs of any march width
         bool fhm = false;     // fh_march_kernel: fused variable-mobility jobs
         long long key = 0;    // launch class (precision, shape class, ring, width)
         int sub = 0;          // index among the groups of one class
@@ -225,15 +224,12 @@ StepKernel step_kernel(bool fp32, bool flat, int nbuf, bool simple, int block, b
 bool nbuf_ok(int nbuf);
 // march step kernels (ch_march.cuh; march_f32.cu, march_f64.cu): periodic,
 // equal spacing, 3-D, row widths up to 256, ring depths 3, 4, 6; nullptr
-// where no variant exists.  order 1 runs both stages between two barriers.
-StepKernel march_kernel_f32(int nx, int nbuf, bool mass, int order);
-StepKernel march_kernel_f64(int nx, int nbuf, int order);
-// one launch for jobs of every march width (ring depths 3 and 6)
-StepKernel march_batch_kernel_f32(int nbuf, bool mass, bool inlined = false);
-StepKernel march_batch_kernel_f64(int nbuf, bool inlined = false);
-bool march_batch_job(const Geometry& g);  // a job the batch kernel takes
-// ring depth of march jobs that share launches (batch, server)
-constexpr int kMarchBatchNbuf = 6;
+// where no variant exists
+StepKernel march_kernel_f32(int nx, int nbuf, bool mass);
+StepKernel march_kernel_f64(int nx, int nbuf);
+// ring depth of 3-D jobs of march widths that share launches (batch, server)
+constexpr int kMarchBatchNbuf = 3;
+bool march_batch_job(const Geometry& g);  // a periodic 3-D job of a march width
 bool geometry_simple(const Geometry& g);
 bool fixed_width_kernel(const Geometry& g, int nbuf);
 int prepare_kernels(const DevInfo& d);

@@ -52,26 +52,27 @@ def test_batch_equals_standalone_bitwise():
         b.close()
 
 
-def test_c4_style_batch_is_one_launch_and_autotune_keeps_results():
-    """FP32 cubic jobs of mixed march widths (64..192) step in ONE persistent
-    launch per step; re-tiling the batch by the autotuner between steps (it
-    may choose a launch per width class) leaves every job bit-identical to
-    its standalone run."""
+def test_c4_style_batch_autotune_keeps_results():
+    """FP32 cubic jobs of mixed march widths (64..192): one launch per width
+    class and step, the classes side by side in one captured graph; re-tiling
+    the batch by the autotuner between steps leaves every job bit-identical
+    to its standalone run."""
     rng = np.random.default_rng(3)
     jobs = []
     for j, e in enumerate((64, 96, 128, 160, 192, 64, 128)):
         p = mb.make_params(e, e, e, 0.005, kappa=float(rng.uniform(0.5, 2.0)), precision="fp32")
         jobs.append((p, mb.ic_generate((e, e, e), float(rng.uniform(-0.4, 0.4)), 0.05, False, 2000 + j)))
+    widths = len({p.nx for p, _ in jobs})
     b = mb.Batch([p for p, _ in jobs])
     try:
         for i, (_, ic) in enumerate(jobs):
             b.set_field(i, ic)
         b.step(12)
-        assert b.info()["launches_per_step"] == 1
+        assert b.info()["launches_per_step"] == widths
         tuned = b.autotune(trials=2)
         assert tuned["threads"] > 0 and tuned["planes"] > 0 and tuned["ms_per_step"] > 0
         b.step(13)
-        assert b.info()["launches_per_step"] <= len({p.nx for p, _ in jobs})
+        assert b.info()["launches_per_step"] <= widths
         for i, (p, ic) in enumerate(jobs):
             want, st = alone(p, ic, 25)
             assert np.array_equal(b.get_field(i), want), i
