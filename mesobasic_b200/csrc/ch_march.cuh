@@ -134,15 +134,29 @@ struct MarchCta {
     uint32_t ph;  // parity of the next completion of each ring slot (bit s)
 };
 
+// shared-memory elements of a c plane and a mu plane: compile-time when the
+// tile height TY is (every job of the launch has it; NXC is a multiple of 32,
+// so the rounded plane of the host equals the product)
+template <int NXC, int TY>
+__device__ __forceinline__ uint32_t march_cplane(const StepArgs& a)
+{
+    return TY ? (uint32_t)((TY + 4) * NXC) : (uint32_t)a.cplane;
+}
+template <int NXC, int TY>
+__device__ __forceinline__ uint32_t march_mplane(const StepArgs& a)
+{
+    return TY ? (uint32_t)((TY + 2) * NXC) : (uint32_t)a.mplane;
+}
+
 template <int NBUF>
-__device__ __forceinline__ MarchCta march_setup(const StepArgs& a, uint32_t es)
+__device__ __forceinline__ MarchCta march_setup(const StepArgs& a, uint32_t es, uint32_t cplane)
 {
     extern __shared__ __align__(128) unsigned char smem_dyn[];
     unsigned char* smem_raw = smem_dyn + ((128u - (smem_addr(smem_dyn) & 127u)) & 127u);
     MarchCta m;
     m.head = reinterpret_cast<SmemHead*>(smem_raw);
     m.cbase = smem_addr(smem_raw) + (uint32_t)(((sizeof(SmemHead) + 127) / 128) * 128);
-    m.mbase = m.cbase + NBUF * (uint32_t)a.cplane * es;
+    m.mbase = m.cbase + NBUF * cplane * es;
     m.bar0 = smem_addr(&m.head->bar[0]);
     m.ph = 0;
     if (threadIdx.x == 0) {
@@ -156,7 +170,7 @@ __device__ __forceinline__ MarchCta march_setup(const StepArgs& a, uint32_t es)
 // One work item (y-tile x z-chunk) of job J, slot `local` among its items.
 // Returns false when a bounded wait ran out (the CTA must exit; the job and
 // the launch are flagged and the copies in flight drained).
-template <typename T, int NXC, int NBUF, bool MASS>
+template <typename T, int NXC, int NBUF, bool MASS, int TY>
 __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int local, MarchCta& cta)
 {
     constexpr int W = Strip<T>::W, HW = W / 2;
@@ -172,7 +186,8 @@ __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int loc
 
     SmemHead* head = cta.head;
     const uint32_t cbase = cta.cbase, mbase = cta.mbase, bar0 = cta.bar0;
-    const uint32_t cplaneB = (uint32_t)a.cplane * ES, mplaneB = (uint32_t)a.mplane * ES;
+    const uint32_t cplaneB = march_cplane<NXC, TY>(a) * ES, mplaneB = march_mplane<NXC, TY>(a) * ES;
+    const int spin = (int)min(a.spin_limit, (long long)0x7fffffff);
     uint32_t& ph = cta.ph;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -203,7 +218,7 @@ __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int loc
         }
 
         const int ny = J->ny, nz = J->nz;
-        const int ty = J->ty;
+        const int ty = TY ? TY : J->ty;
         const double kap = J->kap, dtM = J->dtM;
         const float kapc = (float)(J->kap * J->cx), dtMc = (float)(J->dtM * J->cx);
         const int par = (int)(step & 1);
@@ -280,7 +295,7 @@ __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int loc
         bool failed = false;
         int nw = 0;  // planes this thread has waited for
         auto wait_slot = [&](int s) {
-            if (!mbar_wait_bounded(&head->bar[s], (ph >> s) & 1u, a.spin_limit)) {
+            if (!mbar_wait_bounded32(&head->bar[s], (ph >> s) & 1u, spin)) {
                 failed = true;
                 return;
             }
@@ -403,7 +418,7 @@ __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int loc
                 const int nissued = min(nplanes, ifail >= 2 ? NBUF + ifail : NBUF);
                 for (int p = nw; p < nissued; ++p) {
                     const int s = p % NBUF;
-                    mbar_wait_bounded(&head->bar[s], (ph >> s) & 1u, a.spin_limit);
+                    mbar_wait_bounded32(&head->bar[s], (ph >> s) & 1u, spin);
                     ph ^= 1u << s;
                 }
                 atomicMax(&J->err, DEV_TMA_TIMEOUT);
@@ -455,16 +470,18 @@ __device__ __forceinline__ bool march_item(const StepArgs& a, JobDev* J, int loc
 }
 
 // One job class: every job of the launch has row width NXC.
-template <typename T, int NXC, int NBUF, bool MASS>
+// TY > 0: every job of the launch has tile height TY (its plane sizes and
+// tile geometry are compile-time constants); 0: read from the job.
+template <typename T, int NXC, int NBUF, bool MASS, int TY = 0>
 __global__ void __launch_bounds__(kMaxBlock, 1) ch_march_kernel(StepArgs a)
 {
     step_counts(a);
-    MarchCta cta = march_setup<NBUF>(a, sizeof(T));
+    MarchCta cta = march_setup<NBUF>(a, sizeof(T), march_cplane<NXC, TY>(a));
     for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
         const int j = find_job(a.item_begin, a.njobs, item);
         JobDev* J = a.jobs + __ldg(a.job_slot + j);
         const int local = item - __ldg(a.item_begin + j);
-        if (!march_item<T, NXC, NBUF, MASS>(a, J, local, cta)) return;
+        if (!march_item<T, NXC, NBUF, MASS, TY>(a, J, local, cta)) return;
     }
 }
 

@@ -427,6 +427,12 @@ int prepare_kernels(const DevInfo& d)
                                 MG_CUDA(cudaFuncSetAttribute(step_kernel(f32, fl, nb, sm, bl, ms && f32, fx),
                                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                              (int)d.smem_optin));
+    for (int ms = 0; ms < 2; ++ms)
+        MG_CUDA(cudaFuncSetAttribute(march_kernel_f32(256, 3, ms, 8), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)d.smem_optin));
+    for (int nb : {3, 6})
+        MG_CUDA(cudaFuncSetAttribute(march_kernel_f64(256, nb, 7), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)d.smem_optin));
     MG_CUDA(cudaFuncSetAttribute(fh_march_kernel<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));
     MG_CUDA(cudaFuncSetAttribute(fh_march_kernel<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));
     done = true;
@@ -926,6 +932,13 @@ void Engine::free_graveyard()
 StepKernel Engine::group_kernel(const Group& g) const
 {
     if (g.fhm) return g.flat ? fh_march_kernel<3, true> : fh_march_kernel<3, false>;
+    if (g.simple && !g.flat && g.fixed_nx > 0 && g.fixed_ty > 0 && march_enabled()) {
+        // every job of the group has the same width and tile height: the
+        // variant with both fixed at compile time, where one exists
+        StepKernel k = g.fp32 ? march_kernel_f32(g.fixed_nx, g.nbuf, g.mass, g.fixed_ty)
+                              : march_kernel_f64(g.fixed_nx, g.nbuf, g.fixed_ty);
+        if (k) return k;
+    }
     return step_kernel(g.fp32, g.flat, g.nbuf, g.simple, g.block, g.mass, g.fixed_nx);
 }
 
@@ -1091,8 +1104,11 @@ int Engine::rebuild()
         }
         g.nitems = items;
         g.fixed_nx = g.jobs.front()->g.lnx;
-        for (Job* j : g.jobs)
+        g.fixed_ty = g.jobs.front()->tiling.ty;
+        for (Job* j : g.jobs) {
             if (j->g.lnx != g.fixed_nx) g.fixed_nx = 0;
+            if (j->tiling.ty != g.fixed_ty) g.fixed_ty = 0;
+        }
     }
     // a job-set change that fits the stable lanes: rewrite their tables,
     // keep the graphs

@@ -170,6 +170,7 @@ class Engine {
         std::vector<Job*> jobs;
         int nitems = 0, grid = 0, block = 0;
         int fixed_nx = 0;  // row width shared by every job of the group (0: mixed)
+        int fixed_ty = 0;  // tile height shared by every job of the group (0: mixed)
         size_t smem = 0;
         int cplane = 0, mplane = 0;
         int* d_item_begin = nullptr;
@@ -225,8 +226,10 @@ bool nbuf_ok(int nbuf);
 // march step kernels (ch_march.cuh; march_f32.cu, march_f64.cu): periodic,
 // equal spacing, 3-D, row widths up to 256, ring depths 3, 4, 6; nullptr
 // where no variant exists
-StepKernel march_kernel_f32(int nx, int nbuf, bool mass);
-StepKernel march_kernel_f64(int nx, int nbuf);
+// ty > 0: every job of the launch has tile height ty (a specialised variant
+// where one exists)
+StepKernel march_kernel_f32(int nx, int nbuf, bool mass, int ty = 0);
+StepKernel march_kernel_f64(int nx, int nbuf, int ty = 0);
 // ring depth of 3-D jobs of march widths that share launches (batch, server)
 constexpr int kMarchBatchNbuf = 3;
 bool march_batch_job(const Geometry& g);  // a periodic 3-D job of a march width

@@ -16,8 +16,11 @@ static StepKernel march_f64_nbuf(int nbuf)
     }
 }
 
-StepKernel march_kernel_f64(int nx, int nbuf)
+StepKernel march_kernel_f64(int nx, int nbuf, int ty)
 {
+    // the tile of the 256^3 benchmark shape, specialised
+    if (nx == 256 && ty == 7 && nbuf == 6) return ch_march_kernel<double, 256, 6, false, 7>;
+    if (nx == 256 && ty == 7 && nbuf == 3) return ch_march_kernel<double, 256, 3, false, 7>;
     switch (nx) {
     case 64: return march_f64_nbuf<64>(nbuf);
     case 128: return march_f64_nbuf<128>(nbuf);

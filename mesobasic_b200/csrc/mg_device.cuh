@@ -46,6 +46,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
     return done != 0;
 }
 
+// Bounded wait with a 32-bit poll count (limits up to 2^31 - 1).
+__device__ __forceinline__ bool mbar_wait_bounded32(uint64_t* bar, uint32_t parity, int limit)
+{
+    for (int n = 0; n < limit; ++n)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 // Bounded wait: gives up after `limit` polls and reports false.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit)
 {
