@@ -171,13 +171,13 @@ MODEL_LEG = (
 
 
 def run_models(mb, torch, dev, steps, warmup, flush, sampler, peak):
-    """The variable-mobility steps (FP64, two passes: mu and mobility, then
-    div(mob grad mu) and the update; then the noise term) at 256^3, CUDA
-    events around each step, L2 flushed between steps.  GLUPS counts field
-    site updates (SIPSternary: two fields).  `achieved` is the algorithmic
-    16 B per site update (read c, write c'); the two-pass design moves 56 B
-    (pass 1: read c, write mu and mob; pass 2: read c, mu, mob, write c')
-    plus 16 B for the noise."""
+    """The variable-mobility steps at 256^3 (FP64, the default two passes:
+    mu and 1/mob of every site; then div(mob grad mu), the update and the
+    noise term), CUDA events around each step, L2 flushed between steps.
+    GLUPS counts field site updates (SIPSternary: two fields).  `achieved`
+    is the algorithmic 16 B per site update (read c, write c'); the two
+    passes move 56 B (pass 1: read c, write mu and 1/mob; pass 2: read c,
+    mu, 1/mob, write c')."""
     n = N
     sites = float(n) ** 3
     out = {}
@@ -218,11 +218,10 @@ def run_models(mb, torch, dev, steps, warmup, flush, sampler, peak):
         upd = fields * sites
         out[name] = {"value": upd / (ms * 1e-3) / 1e9, "unit": "GLUPS", "ms_per_step": ms,
                      "achieved_gbs": upd * 16 / (ms * 1e-3) / 1e9, "frac": upd * 16 / (ms * 1e-3) / 1e9 / peak,
-                     "design_gbs": upd * 72 / (ms * 1e-3) / 1e9, "fields": fields}
+                     "design_gbs": upd * 56 / (ms * 1e-3) / 1e9, "fields": fields}
     out["workload"] = (f"{n}^3 FP64 per field, dt 0.01, noise 0.1, {steps} timed steps after {warmup} warm-up, "
                        "L2 flushed between steps; TIPSphil periodic, the others no-flux x")
-    out["bytes"] = ("achieved: 16 B per site update (algorithmic); design_gbs: 72 B per site update "
-                    "(two passes 56 B + noise 16 B)")
+    out["bytes"] = "achieved: 16 B per site update (algorithmic); design_gbs: 56 B per site update (two passes)"
     return out
 
 

@@ -150,7 +150,10 @@ void* mg_ch_field_device(mg_ch_t* h);
 long long mg_ch_steps(mg_ch_t* h);
 
 int mg_ch_get_tiling(const mg_ch_t* h, mg_tiling* out);
-/* Overrides the decomposition; validates it against the kernel limits. */
+/* Overrides the decomposition; validates it against the kernel limits.
+ * Variable-mobility handles step on two per-site passes (path 1) by default;
+ * path 0 selects the fused z-marching kernel (ty 0: its own tile choice),
+ * which gives the same field bit for bit. */
 int mg_ch_set_tiling(mg_ch_t* h, const mg_tiling* t);
 
 /* Frees the device buffers.  Replaces: PFApp::~PFApp (PFApp.cpp:69-72). */

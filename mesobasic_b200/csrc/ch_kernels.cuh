@@ -670,20 +670,15 @@ __global__ void fh_mu_mob_kernel(JobDev* job)
 // SfieldFD.cpp:333-355) from mu and the reciprocal mobilities of pass 1:
 // each face's harmonic mean 2/(1/mob_a + 1/mob_b) from the two stored
 // reciprocals -- the reference's operands in its order, so the same value.
-__global__ void fh_update_kernel(JobDev* job)
+// Then the per-step noise (TIPSphil.cpp:200-209), as ch_noise_kernel adds
+// it: a thread takes four consecutive sites, one draw of the counter-based
+// generator (site/4, step).
+__device__ __forceinline__ double fh_update_site(const JobDev& J, const double* __restrict__ c,
+                                                 const double* __restrict__ mu, const double* __restrict__ rmob,
+                                                 size_t s)
 {
     using A = Arith<double>;
-    const JobDev& J = *job;
-    const FhDev& F = *J.fh;
     const int nx = J.nx, ny = J.ny, nz = J.nz;
-    const size_t n = (size_t)nx * ny * nz;
-    const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (J.step >= J.target || s >= n) return;
-    const int par = (int)(J.step & 1);
-    const double* __restrict__ c = static_cast<const double*>(J.buf[par]);
-    double* __restrict__ out = static_cast<double*>(J.buf[par ^ 1]);
-    const double* __restrict__ mu = F.mu;
-    const double* __restrict__ rmob = F.mob;
     const int x = (int)(s % nx), y = (int)((s / nx) % ny), z = (int)(s / ((size_t)nx * ny));
     const bool pX = J.flags & JF_PER_X, pY = J.flags & JF_PER_Y, pZ = J.flags & JF_PER_Z;
     const double a0 = mu[s], ro = rmob[s];
@@ -699,7 +694,41 @@ __global__ void fh_update_kernel(JobDev* job)
         const double ly = fh_axis_r(mu[iym], mu[iyp], a0, rmob[iym], rmob[iyp], ro, J.cy, J.flags & JF_DIV_Y);
         lap = A::add(A::add(lx, ly), lz);
     }
-    out[s] = A::add(c[s], A::mul(J.dtM_dt, lap));  // c += dt * lap (TIPSphil.cpp:194)
+    return A::add(c[s], A::mul(J.dtM_dt, lap));  // c += dt * lap (TIPSphil.cpp:194)
+}
+
+__global__ void fh_update_kernel(JobDev* job)
+{
+    using A = Arith<double>;
+    const JobDev& J = *job;
+    const FhDev& F = *J.fh;
+    const long long n = (long long)J.nx * J.ny * J.nz;
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // sites 4g .. 4g+3
+    if (J.step >= J.target || 4 * g >= n) return;
+    const int par = (int)(J.step & 1);
+    const double* __restrict__ c = static_cast<const double*>(J.buf[par]);
+    double* __restrict__ out = static_cast<double*>(J.buf[par ^ 1]);
+    uint32_t word[4] = {0u, 0u, 0u, 0u};
+    const bool noisy = J.noise != 0.0;
+    if (noisy) {
+        const long long st = J.step + 1;  // the step being taken
+        const uint2 key = make_uint2((uint32_t)J.noise_seed, (uint32_t)(J.noise_seed >> 32));
+        const uint4 w = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)(g >> 32), (uint32_t)st, (uint32_t)(st >> 32)), key);
+        word[0] = w.x, word[1] = w.y, word[2] = w.z, word[3] = w.w;
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const long long s = 4 * g + e;
+        if (s >= n) break;
+        double v = fh_update_site(J, c, F.mu, F.mob, (size_t)s);
+        if (noisy) {
+            // SIPS.cpp:239-240: no noise at or above the cutoff (+inf elsewhere)
+            const double r = A::add(A::mul((double)word[e], 2.3283064365386963e-10), 1.1641532182693481e-10);
+            const double val = v >= J.noise_cutoff ? 0.0 : A::mul(J.noise, A::sub(r, 0.5));
+            v = A::add(v, A::mul(J.dtM_dt, val));
+        }
+        out[s] = v;
+    }
 }
 
 // advances the step counter after a generic-path step

@@ -775,7 +775,10 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const Fh
     if (fh) {
         // the fused variable-mobility kernel where the shape allows, else the
         // per-site path (path 1)
-        j->tiling = mg_env_int("MG_FH_FUSED", 1) == 1 ? fh_default_tiling(j->g, info) : mg_tiling{1, 1, 4, 1};
+        // the two-pass kernels (path 1) by default: the step is bound by
+        // FP64 arithmetic, where their occupancy beats the fused kernel's
+        // (path 0, fh_march_kernel, chosen with mg_ch_set_tiling)
+        j->tiling = mg_tiling{1, 1, 4, 1};
         MG_TRY(plan_fh_tiling(j->g, j->tiling, info, &j->plan));
     } else {
         j->tiling = batch_tiling ? batch_tiling_for(j->g, info, device, batch_threads, batch_planes)
@@ -859,15 +862,19 @@ void Engine::remove_job(Job* j)
 int Engine::set_tiling(Job* j, const mg_tiling& t)
 {
     TilePlan pl;
-    if (j->d_fh) MG_TRY(plan_fh_tiling(j->g, t, info, &pl));
-    else MG_TRY(plan_tiling(j->g, t, info, &pl));
+    mg_tiling t_in = t;
+    // variable mobility: path 0 with ty 0 asks for the fused kernel's own tiling
+    if (j->d_fh && t.path == 0 && t.ty == 0) t_in = fh_default_tiling(j->g, info);
+    const mg_tiling& tt = t_in;
+    if (j->d_fh) MG_TRY(plan_fh_tiling(j->g, tt, info, &pl));
+    else MG_TRY(plan_tiling(j->g, tt, info, &pl));
     if (j->p.mass_correct && !pl.tma_ok) return fail(MG_EINVAL, "mass_correct needs the tiled kernel");
     MG_CUDA(cudaStreamSynchronize(stream));
     long long* part = nullptr;
     MG_CUDA(cudaMalloc(&part, sizeof(long long) * std::max(pl.nitems, 1)));
     const mg_tiling old = j->tiling;
     const TilePlan old_plan = j->plan;
-    j->tiling = t;
+    j->tiling = tt;
     j->plan = pl;
     if (pl.tma_ok) {
         // new maps at a new address: a launch never sees a map rewritten in place
@@ -1197,7 +1204,7 @@ int Engine::launch_lane(const Group& g, Job* generic_job, cudaStream_t st)
             long long q = std::max(1LL, 8LL * info.sms * 256 / l);
             q = std::min(q, std::max(1LL, (long long)((j->g.n + l - 1) / l)));
             fh_mu_mob_kernel<<<(unsigned)(l * q / 256), 256, 0, st>>>(d_jobs_ + j->slot);
-            fh_update_kernel<<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
+            fh_update_kernel<<<(unsigned)((j->g.n / 4 + 256) / 256), 256, 0, st>>>(d_jobs_ + j->slot);
         } else if (g.fp32) {
             ch_step_generic_kernel<float><<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
         } else {
@@ -1226,9 +1233,13 @@ int Engine::launch_lane(const Group& g, Job* generic_job, cudaStream_t st)
         if (g.fp32) ch_noise_kernel<float><<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
         else ch_noise_kernel<double><<<blocks, 256, 0, st>>>(d_jobs_ + j->slot);
     };
-    if (g.generic) noise(generic_job);
-    else if (!g.fhm)  // the fused variable-mobility kernel adds its noise itself
+    // variable-mobility steps add their noise themselves (fh_update_kernel,
+    // fh_march_kernel)
+    if (g.generic) {
+        if (!generic_job->d_fh) noise(generic_job);
+    } else if (!g.fhm) {
         for (Job* j : g.jobs) noise(j);
+    }
     MG_CUDA(cudaGetLastError());
     return MG_OK;
 }

@@ -167,3 +167,26 @@ noiseStr = 0
     assert t0[12] == "460.000"
     t20 = [float(v) for v in (tmp_path / "vtkoutput" / "temp_20.vtk").read_text().splitlines()[12:12 + 32]]
     assert 260.0 < t20[0] < t20[-1] <= 320.0  # warmer away from the bath at x = 0
+
+
+@pytest.mark.parametrize("dims,bc,sips", [((32, 20, 16), (1, 1, 1), False), ((32, 12, 10), (0, 0, 1), False),
+                                          ((48, 36, 1), (1, 0, 1), False), ((32, 16, 12), (0, 1, 1), True)])
+def test_fused_kernel_bit_identical_to_two_pass(oracle, dims, bc, sips):
+    """The fused z-marching variable-mobility kernel (fh_march_kernel, tiling
+    path 0) and the two-pass kernels (the default) take the same operations
+    in the same order, noise included: their fields agree bit for bit."""
+    ic = oracle.ic(dims, 0.3, 0.1, False, 5)
+    p = mb.make_params(*dims, 0.01, bc=bc, noise=0.1, noise_seed=9)
+    kw = dict(sips=mb.make_sips_params(Mweight=1.0, Mvolume=1.0, gamma=1.0)) if sips else \
+        dict(fh=mb.make_fh_params(50, **QUENCH))
+    out = []
+    for fused in (False, True):
+        with mb.CHSim(p, **kw) as sim:
+            if fused:
+                sim.tiling = (0, 0, 3, 0)  # path 0, ty 0: the fused kernel's own tiling
+                assert sim.tiling.path == 0 and sim.tiling.ty >= 1
+            sim.set_field(ic)
+            sim.step(12)
+            out.append(sim.get_field())
+    assert np.array_equal(out[0], out[1])
+    assert np.abs(out[1] - ic).max() > 1e-4
