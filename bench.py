@@ -40,8 +40,8 @@ CONFIG = {"workload": "3-D Cahn-Hilliard 256^3 explicit step, dt 0.005, M 1, kap
 METRIC = "GLUPS & % HBM roofline (FP32 vs FP64)"
 # DRAM traffic per launch is read from the committed ncu summaries (one
 # capture of the same kernel and tiling), not measured inside this run
-TRAFFIC_SOURCE = {"fp64": "ncu capture in profiles/ncu_ch_step_fp64_256.md (same kernel and tiling)",
-                  "fp32": "ncu capture in profiles/ncu_ch_step_fp32_256.md (same kernel and tiling)"}
+TRAFFIC_SOURCE = {"fp64": "ncu capture in profiles/ncu_ch_march_fp64_256.md (same kernel and tiling)",
+                  "fp32": "ncu capture in profiles/ncu_ch_march_fp32_256.md (same kernel and tiling)"}
 
 
 def load_peaks():
@@ -55,7 +55,7 @@ def load_peaks():
 
 def load_traffic(dtype):
     """DRAM bytes per launch of the step kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", f"ncu_ch_step_{dtype}_256.md")
+    p = os.path.join(ROOT, "profiles", f"ncu_ch_march_{dtype}_256.md")
     if not os.path.exists(p):
         return None
     for line in open(p):

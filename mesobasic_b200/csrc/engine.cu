@@ -428,10 +428,14 @@ int prepare_kernels(const DevInfo& d)
                                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                              (int)d.smem_optin));
     for (int ms = 0; ms < 2; ++ms)
-        MG_CUDA(cudaFuncSetAttribute(march_kernel_f32(256, 3, ms, 8), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)d.smem_optin));
+        for (int ty : {4, 6, 8})
+            MG_CUDA(cudaFuncSetAttribute(march_kernel_f32(256, 3, ms, ty), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)d.smem_optin));
     for (int nb : {3, 6})
         MG_CUDA(cudaFuncSetAttribute(march_kernel_f64(256, nb, 7), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)d.smem_optin));
+    for (int ty : {4, 5, 6})
+        MG_CUDA(cudaFuncSetAttribute(march_kernel_f64(256, 3, ty), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)d.smem_optin));
     MG_CUDA(cudaFuncSetAttribute(fh_march_kernel<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));
     MG_CUDA(cudaFuncSetAttribute(fh_march_kernel<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));
@@ -1022,10 +1026,10 @@ int Engine::rebuild()
 {
     MG_CUDA(cudaStreamSynchronize(stream));
     free_graveyard();
-    // Several jobs: one ring depth per class (4 planes for 3-D jobs, 8 for
-    // 2-D) so that each class steps in one launch.  Only nbuf changes; the
-    // tile rows and z chunks, which fix a job's reduction order and so its
-    // results, stay as chosen.
+    // Several jobs: one ring depth per class (3 planes for 3-D jobs of a
+    // march width, 4 for other 3-D jobs, 8 for 2-D) so that each class steps
+    // in one launch.  Only nbuf changes; the tile rows and z chunks, which
+    // fix a job's reduction order and so its results, stay as chosen.
     const bool shared = jobs.size() > 1 || stable_lanes;  // launches shared by several jobs
     if (shared)
         for (Job* j : jobs) {
