@@ -330,10 +330,39 @@ def run_precision(mb, dev, steps, n=512, seed=42, every=250):
     return out
 
 
-def run_serve(mb, dev, window_s, seed=11, rate=20.0, burst=0):
+def batch_same_mix(mb, torch, dev, arrivals, noise, steps=100, warmup=10):
+    """The served burst's jobs (same shapes, precisions, parameters and
+    fields) stepped together as one batch, `steps` steps timed by CUDA
+    events on the batch's stream: what the batch path gives on the served
+    mix, against which the served throughput is compared."""
+    params = [mb.make_params(*dims, dt, kappa=kap, precision=prec) for (_, dims, dt, prec, _, kap, _, _) in arrivals]
+    b = mb.Batch(params, dev)
+    try:
+        for j, (_, dims, _, _, c0, _, _, _) in enumerate(arrivals):
+            b.set_field(j, noise[dims] + c0)
+        b.step(warmup)
+        b.sync()
+        ext = torch.cuda.ExternalStream(b.stream, device=f"cuda:{dev}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(ext)
+        b.step(steps)
+        e1.record(ext)
+        b.sync()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        launches = b.info()["launches_per_step"]
+    finally:
+        b.close()
+    sites = float(sum(d[0] * d[1] * d[2] for (_, d, *_r) in arrivals))
+    return {"glups": sites * steps / (ms * 1e-3) / 1e9, "steps": steps, "launches_per_step": launches}
+
+
+def run_serve(mb, dev, window_s, seed=11, rate=20.0, burst=0, torch=None):
     """Served stream: Poisson arrivals at `rate` jobs/s for `window_s` seconds, then drain.
     burst > 0: that many jobs of the same mix submitted at once (the queue
-    never runs dry: the server's saturated throughput)."""
+    never runs dry: the server's saturated throughput); with `torch` the
+    same jobs are then stepped as one batch for comparison."""
     import numpy as np
     rng = np.random.default_rng(seed)
     arrivals, t = [], 0.0
@@ -378,6 +407,7 @@ def run_serve(mb, dev, window_s, seed=11, rate=20.0, burst=0):
         st = srv.stats()
     finally:
         srv.close()
+    same_mix = batch_same_mix(mb, torch, dev, arrivals, noise) if (burst and torch is not None) else None
     upd = sum(d[0] * d[1] * d[2] * n for (_, d, _, _, _, _, n, _) in arrivals)
     upd_bytes = sum(d[0] * d[1] * d[2] * n * (8 if pr == "fp32" else 16) for (_, d, _, pr, _, _, n, _) in arrivals)
     return {"sims_per_hour": st["sims_per_hour"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
@@ -386,7 +416,7 @@ def run_serve(mb, dev, window_s, seed=11, rate=20.0, burst=0):
             "worker_s": {k: st[k] for k in ("step_s", "admit_s", "retire_s")},
             "ticks": st["ticks"], "rebuilds": st["rebuilds"], "refreshes": st["refreshes"],
             "glups": st["site_updates_per_s"] / 1e9, "hbm_peak_gb": st["hbm_peak_gb"], "wall_s": wall,
-            "submitted": len(arrivals),
+            "submitted": len(arrivals), "batch_same_mix": same_mix,
             "workload": (f"{burst} jobs submitted at once (seed {seed})" if burst else
                          f"Poisson arrivals {rate:g}/s for {window_s:g} s (seed {seed})") + ": 50% 2-D edge "
                         "{128,256,512,1024} dt 0.01, 50% 3-D edge {64..256 step 32} dt 0.005, 50/50 fp32/fp64, "
@@ -502,13 +532,19 @@ def run_ours(args, rank, world, local_rank):
         serve["reported"] = f"median of {len(runs)} runs by sims_per_hour"
         if args.serve_burst > 0:
             # saturated: a burst of the same mix, the queue never empty
-            sat = run_serve(mb, dev, args.serve_seconds, burst=args.serve_burst)
+            sat = run_serve(mb, dev, args.serve_seconds, burst=args.serve_burst, torch=torch)
             serve["saturated"] = {k: sat[k] for k in ("glups", "sims_per_hour", "p50_ms", "p99_ms", "completed",
                                                       "ticks", "rebuilds", "refreshes", "wall_s")}
             # the fraction uses the mix's algorithmic bytes (8 B per FP32
             # site update, 16 B per FP64)
             serve["saturated"]["roofline_frac"] = sat["gbs"] / peak
             serve["saturated"]["vs_batch"] = sat["glups"] / batch["value"] if batch else None
+            # against the batch path on the same jobs (mixed precisions, 2-D
+            # and 3-D): the server's own overhead (ticks, admission, retiring,
+            # the drain) without the difference in workload
+            bm = sat["batch_same_mix"]
+            serve["saturated"]["batch_same_mix_glups"] = bm["glups"]
+            serve["saturated"]["vs_batch_same_mix"] = sat["glups"] / bm["glups"]
             serve["saturated"]["workload"] = sat["workload"]
     if batch and dist:
         tt = torch.tensor([batch["ms"]], device=f"cuda:{dev}", dtype=torch.float64)
@@ -573,7 +609,9 @@ def run_ours(args, rank, world, local_rank):
         "serve": None if not serve else {
             "sims_per_hour": serve["sims_per_hour"], "p50_ms": serve["p50_ms"], "p99_ms": serve["p99_ms"],
             "glups": serve["glups"], "runs": len(serve["runs"]), "reported": serve["reported"],
-            "saturated": serve.get("saturated")},
+            "saturated": None if not serve.get("saturated") else
+            {k: v for k, v in serve["saturated"].items() if k != "workload"}
+            | {"workload": f"burst of {args.serve_burst} jobs of the same mix (detail file)"}},
         "precision": None if not precision else {
             k: precision.get(k) for k in ("maxnorm_fp32_vs_fp64", "mass_drift_rel_fp32", "mass_drift_rel_fp64",
                                           "sk_peak_rel_diff", "energy_rel_diff_max")},

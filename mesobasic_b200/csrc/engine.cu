@@ -428,14 +428,10 @@ int prepare_kernels(const DevInfo& d)
                                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                              (int)d.smem_optin));
     for (int ms = 0; ms < 2; ++ms)
-        for (int ty : {4, 6, 8})
-            MG_CUDA(cudaFuncSetAttribute(march_kernel_f32(256, 3, ms, ty), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)d.smem_optin));
+        MG_CUDA(cudaFuncSetAttribute(march_kernel_f32(256, 3, ms, 8), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)d.smem_optin));
     for (int nb : {3, 6})
         MG_CUDA(cudaFuncSetAttribute(march_kernel_f64(256, nb, 7), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)d.smem_optin));
-    for (int ty : {4, 5, 6})
-        MG_CUDA(cudaFuncSetAttribute(march_kernel_f64(256, 3, ty), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)d.smem_optin));
     MG_CUDA(cudaFuncSetAttribute(fh_march_kernel<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));
     MG_CUDA(cudaFuncSetAttribute(fh_march_kernel<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));

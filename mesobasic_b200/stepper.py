@@ -5,6 +5,11 @@ GLUPS.  Used for quick measurements, tiling sweeps and profiler captures.
     python -m mesobasic_b200.stepper --n 256 --tiling 8,8,6 --steps 20
     python -m mesobasic_b200.stepper --n 256 --autotune
     python -m mesobasic_b200.stepper --n 256 --sweep   # every valid tiling, sorted
+    python -m mesobasic_b200.stepper --n 256 --model tipsphil --steps 4
+
+--model tipsphil runs the variable-mobility TIPSphil step (FP64, periodic,
+dt 0.01, noise 0.1, c = 0.3 + U[-0.05, 0.05]) with the quench of the
+models leg of the benchmark.
 """
 from __future__ import annotations
 
@@ -32,7 +37,13 @@ def parse():
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--sweep", action="store_true")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--model", choices=["ch", "tipsphil"], default="ch")
     return ap.parse_args()
+
+
+# TIPSphil quench of the benchmark's models leg
+TIPSPHIL = dict(alpha=150.0, beta=0.1, N=50.0, Tinit=300.0, Tbath=280.0, Tcrystal=200.0, gamma=1.0, D0=1.0,
+                Mweight=0.5, Mvolume=1.0)
 
 
 def time_steps(sim, steps, warmup):
@@ -51,6 +62,14 @@ def main():
     sites = float(np.prod(dims))
     bytes_site = 16 if a.precision == "fp64" else 8
     ic = mb.ic_generate(dims, 0.0, 0.1, False, 42)
+    if a.model == "tipsphil":
+        p = mb.make_params(*dims, 0.01, noise=0.1, noise_seed=42)
+        with mb.CHSim(p, a.device, fh=mb.make_fh_params(10 ** 6, **TIPSPHIL)) as sim:
+            sim.set_field(0.3 + ic)
+            s = time_steps(sim, a.steps, a.warmup)
+            print(json.dumps({"dims": dims, "model": "TIPSphil", "tiling": sim.tiling.as_tuple(),
+                              "ms_per_step": s * 1e3, "glups": sites / s * 1e-9}))
+        return
     if a.autotune:
         t, ms = mb.autotune(p, a.device, trials=max(5, a.steps))
         print(json.dumps({"autotune": t.as_tuple(), "ms": ms, "glups": sites / ms * 1e-6}))
