@@ -748,9 +748,9 @@ int Engine::init(int dev, int capacity)
     MG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     capacity_ = capacity;
     MG_CUDA(cudaMalloc(&d_jobs_, sizeof(JobDev) * capacity));
-    MG_CUDA(cudaMemset(d_jobs_, 0, sizeof(JobDev) * capacity));
+    MG_CUDA(cudaMemsetAsync(d_jobs_, 0, sizeof(JobDev) * capacity, stream));
     MG_CUDA(cudaMalloc(&d_err_, sizeof(int)));
-    MG_CUDA(cudaMemset(d_err_, 0, sizeof(int)));
+    MG_CUDA(cudaMemsetAsync(d_err_, 0, sizeof(int), stream));
     MG_CUDA(cudaMalloc(&d_diag_part_, sizeof(double2) * 3 * kDiagBlocks));
     MG_CUDA(cudaMalloc(&d_diag_max_, sizeof(double) * kDiagBlocks));
     MG_CUDA(cudaMalloc(&d_diag_bad_, sizeof(double) * kDiagBlocks));
@@ -801,7 +801,7 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const Fh
             FhDev f = *fh;
             f.mu = j->d_mu;
             f.mob = j->d_mob;
-            e = cudaMemcpy(j->d_fh, &f, sizeof f, cudaMemcpyHostToDevice);
+            e = cudaMemcpyAsync(j->d_fh, &f, sizeof f, cudaMemcpyHostToDevice, stream);
         }
     }
     if (e != cudaSuccess) {
@@ -820,7 +820,7 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const Fh
         CUtensorMap maps[4];
         int rc = encode_maps(*j, maps);
         if (rc == MG_OK) {
-            cudaError_t ce = cudaMemcpy(j->d_tmap, maps, sizeof maps, cudaMemcpyHostToDevice);
+            cudaError_t ce = cudaMemcpyAsync(j->d_tmap, maps, sizeof maps, cudaMemcpyHostToDevice, stream);
             if (ce != cudaSuccess) rc = fail(MG_ECUDA, "copying tensor maps: %s", cudaGetErrorString(ce));
         }
         if (rc != MG_OK) {
@@ -838,7 +838,7 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const Fh
     free_slots_.pop_back();
     JobDev jd;
     fill_jobdev(*j, &jd);
-    MG_CUDA(cudaMemcpy(d_jobs_ + j->slot, &jd, sizeof jd, cudaMemcpyHostToDevice));
+    MG_CUDA(cudaMemcpyAsync(d_jobs_ + j->slot, &jd, sizeof jd, cudaMemcpyHostToDevice, stream));
     jobs.push_back(j.get());
     dirty_ = true;
     *out = j.release();
@@ -883,7 +883,7 @@ int Engine::set_tiling(Job* j, const mg_tiling& t)
         int rc = encode_maps(*j, maps);
         if (rc == MG_OK) {
             cudaError_t e = cudaMalloc(&d_new, sizeof maps);
-            if (e == cudaSuccess) e = cudaMemcpy(d_new, maps, sizeof maps, cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(d_new, maps, sizeof maps, cudaMemcpyHostToDevice, stream);
             if (e != cudaSuccess) rc = fail(MG_ECUDA, "tensor maps: %s", cudaGetErrorString(e));
         }
         if (rc != MG_OK) {
@@ -909,7 +909,7 @@ int Engine::set_tiling(Job* j, const mg_tiling& t)
     jd.step = h_state_->step;
     jd.target = h_state_->target;
     jd.err = h_state_->err;
-    MG_CUDA(cudaMemcpy(d_jobs_ + j->slot, &jd, sizeof jd, cudaMemcpyHostToDevice));
+    MG_CUDA(cudaMemcpyAsync(d_jobs_ + j->slot, &jd, sizeof jd, cudaMemcpyHostToDevice, stream));
     dirty_ = true;
     return MG_OK;
 }
@@ -950,7 +950,12 @@ StepKernel Engine::group_kernel(const Group& g) const
 }
 
 // The job list, item offsets and (stable lanes) counts of a group, written
-// to its device tables.
+// to its device tables.  Every host-to-device write of engine metadata (job
+// slots, launch tables, tensor maps) is ordered on the engine's stream: a
+// synchronous cudaMemcpy from pageable memory may return before its DMA has
+// landed, and the engine's non-blocking stream is not ordered after the
+// legacy stream, so the next kernel could read the old contents (a recycled
+// slot's buffers, a tensor map not yet written).
 int Engine::write_tables(const Group& g)
 {
     std::vector<int> begin, slot;
@@ -962,11 +967,12 @@ int Engine::write_tables(const Group& g)
     }
     begin.push_back(items);
     if ((int)slot.size() > g.table_cap) return fail(MG_EINVAL, "launch table holds %d jobs, not %zu", g.table_cap, slot.size());
-    MG_CUDA(cudaMemcpy(g.d_item_begin, begin.data(), sizeof(int) * begin.size(), cudaMemcpyHostToDevice));
-    if (!slot.empty()) MG_CUDA(cudaMemcpy(g.d_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice));
+    MG_CUDA(cudaMemcpyAsync(g.d_item_begin, begin.data(), sizeof(int) * begin.size(), cudaMemcpyHostToDevice, stream));
+    if (!slot.empty())
+        MG_CUDA(cudaMemcpyAsync(g.d_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice, stream));
     if (g.d_counts) {
         const int counts[2] = {(int)g.jobs.size(), items};
-        MG_CUDA(cudaMemcpy(g.d_counts, counts, sizeof counts, cudaMemcpyHostToDevice));
+        MG_CUDA(cudaMemcpyAsync(g.d_counts, counts, sizeof counts, cudaMemcpyHostToDevice, stream));
     }
     return MG_OK;
 }
