@@ -455,6 +455,13 @@ __device__ __forceinline__ FhCol fh_column(const FhDev& F, int x, double cs, dou
     return k;
 }
 
+// x^nu of the Phillies mobility.  x^1 is x exactly (the reference's
+// default nu = 1), which spares the general pow.
+__device__ __forceinline__ double fh_pow(double x, double nu)
+{
+    return nu == 1.0 ? x : pow(x, nu);
+}
+
 // mu and mobility of one site from its concentration cc, its Laplacian
 // lapc and the column constants k, every operation rounded on its own in
 // the reference's order: TIPSphil.cpp:135-177 (and TIPSbathPHIL's),
@@ -483,7 +490,7 @@ __device__ __forceinline__ void fh_site_col(const FhDev& F, const FhCol& k, doub
         else cphil = A::div(A::mul(cc, F.Mweight), F.Mvolume);
         double ddf = A::mul(0.5, A::add(A::div(1.0, A::mul(F.N, cc)), A::div(1.0, A::sub(1.0, cc))));
         ddf = A::mul(ddf, k.kT);
-        const double Dp = A::mul(F.D0, exp(A::mul(-F.gamma, pow(cphil, F.nu))));
+        const double Dp = A::mul(F.D0, exp(A::mul(-F.gamma, fh_pow(cphil, F.nu))));
         double Mc = A::div(Dp, ddf);
         if (Mc > 1.0) Mc = 1.0;
         else if (Mc < 0.00001) Mc = 0.00001;
@@ -510,7 +517,7 @@ __device__ __forceinline__ void fh_site_col(const FhDev& F, const FhCol& k, doub
         ddf = A::mul(0.5, A::add(A::div(1.0, A::mul(F.N, cc)), A::div(1.0, A::sub(1.0, cc))));
     }
     ddf = A::mul(ddf, k.kT);
-    const double Dp = A::mul(k.D, exp(A::mul(-F.gamma, pow(cc_phil, F.nu))));
+    const double Dp = A::mul(k.D, exp(A::mul(-F.gamma, fh_pow(cc_phil, F.nu))));
     double Mc = A::div(Dp, ddf);
     if (Mc < 0.000001) Mc = 0.000001;
     if (Mc > F.D0) Mc = F.D0;

@@ -646,8 +646,12 @@ __global__ void fh_mu_mob_kernel(JobDev* job)
     const size_t stride = (size_t)gridDim.x * blockDim.x;  // a multiple of nx (the host's launch)
     const int x = (int)(first % nx);
     const FhCol col = fh_column(F, x, cs, J.dtM_dt);
+    // the row (y, z) of site s, advanced by the stride's whole rows without
+    // a division per site
+    const size_t r0 = first / nx, dr = stride / nx;
+    int y = (int)(r0 % ny), z = (int)(r0 / ny);
+    const int dy = (int)(dr % ny), dz = (int)(dr / ny);
     for (size_t s = first; s < n; s += stride) {
-        const int y = (int)((s / nx) % ny), z = (int)(s / ((size_t)nx * ny));
         const double cc = c[s];
         const double xp = c[fh_at(wrap_or_clamp(x + 1, nx, pX), y, z, J)], xm = c[fh_at(wrap_or_clamp(x - 1, nx, pX), y, z, J)];
         const double zp = c[fh_at(x, y, wrap_or_clamp(z + 1, nz, pZ), J)], zm = c[fh_at(x, y, wrap_or_clamp(z - 1, nz, pZ), J)];
@@ -663,6 +667,12 @@ __global__ void fh_mu_mob_kernel(JobDev* job)
         fh_site_col(F, col, cc, lapc, J.kap, &mu, &mob);
         F.mu[s] = mu;
         F.mob[s] = A::div(1.0, mob);  // the reciprocal every face of the site uses
+        y += dy;
+        z += dz;
+        if (y >= ny) {
+            y -= ny;
+            z += 1;
+        }
     }
 }
 
@@ -675,11 +685,10 @@ __global__ void fh_mu_mob_kernel(JobDev* job)
 // generator (site/4, step).
 __device__ __forceinline__ double fh_update_site(const JobDev& J, const double* __restrict__ c,
                                                  const double* __restrict__ mu, const double* __restrict__ rmob,
-                                                 size_t s)
+                                                 size_t s, int x, int y, int z)
 {
     using A = Arith<double>;
     const int nx = J.nx, ny = J.ny, nz = J.nz;
-    const int x = (int)(s % nx), y = (int)((s / nx) % ny), z = (int)(s / ((size_t)nx * ny));
     const bool pX = J.flags & JF_PER_X, pY = J.flags & JF_PER_Y, pZ = J.flags & JF_PER_Z;
     const double a0 = mu[s], ro = rmob[s];
     const size_t ixm = fh_at(wrap_or_clamp(x - 1, nx, pX), y, z, J), ixp = fh_at(wrap_or_clamp(x + 1, nx, pX), y, z, J);
@@ -716,11 +725,21 @@ __global__ void fh_update_kernel(JobDev* job)
         const uint4 w = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)(g >> 32), (uint32_t)st, (uint32_t)(st >> 32)), key);
         word[0] = w.x, word[1] = w.y, word[2] = w.z, word[3] = w.w;
     }
+    // coordinates of the first site; the others follow along x
+    const long long s0 = 4 * g, r0 = s0 / J.nx;
+    int x = (int)(s0 - r0 * J.nx), y = (int)(r0 % J.ny), z = (int)(r0 / J.ny);
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-        const long long s = 4 * g + e;
+        const long long s = s0 + e;
         if (s >= n) break;
-        double v = fh_update_site(J, c, F.mu, F.mob, (size_t)s);
+        if (e > 0 && ++x == J.nx) {
+            x = 0;
+            if (++y == J.ny) {
+                y = 0;
+                ++z;
+            }
+        }
+        double v = fh_update_site(J, c, F.mu, F.mob, (size_t)s, x, y, z);
         if (noisy) {
             // SIPS.cpp:239-240: no noise at or above the cutoff (+inf elsewhere)
             const double r = A::add(A::mul((double)word[e], 2.3283064365386963e-10), 1.1641532182693481e-10);
