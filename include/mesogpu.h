@@ -112,7 +112,10 @@ int mg_ch_set_field(mg_ch_t* h, const double* host);
 int mg_ch_step(mg_ch_t* h, int nsteps);
 
 /* Waits for the enqueued work, at most timeout_us microseconds (<0: no
- * limit); reports kernel-side errors.  Replaces: MPI Barrier after a
+ * limit); reports kernel-side errors.  After it has returned MG_EDEVICE
+ * (a bounded device wait ran out, so copies may have been in flight when
+ * the kernel gave up) the handle refuses further steps with MG_EDEVICE:
+ * destroy it and create a new one.  Replaces: MPI Barrier after a
  * step (TIPSphil.cpp:129,192) as the completion point. */
 int mg_ch_sync(mg_ch_t* h, long long timeout_us);
 

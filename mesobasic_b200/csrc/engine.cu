@@ -1317,6 +1317,8 @@ static int graph_steps()
 int Engine::enqueue_steps(int nsteps)
 {
     if (nsteps < 0) return fail(MG_EINVAL, "nsteps must be >= 0");
+    if (poisoned_)
+        return fail(MG_EDEVICE, "an earlier step reported a device error; this handle takes no further steps");
     MG_CUDA(cudaSetDevice(device));
     if (dirty_) MG_TRY(rebuild());
     if (jobs.empty()) return MG_OK;
@@ -1353,7 +1355,12 @@ int Engine::sync(long long timeout_us)
     }
     int err = 0;
     MG_CUDA(cudaMemcpy(&err, d_err_, sizeof err, cudaMemcpyDeviceToHost));
-    if (err != DEV_OK) return fail(MG_EDEVICE, "a step kernel reported device error %d (TMA wait ran out)", err);
+    if (err != DEV_OK) {
+        // a bounded wait ran out: copies may still have been in flight when
+        // the CTA gave up, so the fields and the ring state are not trusted
+        poisoned_ = true;
+        return fail(MG_EDEVICE, "a step kernel reported device error %d (TMA wait ran out)", err);
+    }
     return MG_OK;
 }
 

@@ -206,6 +206,7 @@ class Engine {
     int capacity_ = 0;
     JobDev* d_jobs_ = nullptr;
     int* d_err_ = nullptr;
+    bool poisoned_ = false;  // a kernel reported a device error: no further steps
     std::vector<int> free_slots_;
     std::vector<Group> groups_;
     bool dirty_ = true;
@@ -229,6 +230,8 @@ bool nbuf_ok(int nbuf);
 // ty > 0: every job of the launch has tile height ty (a specialised variant
 // where one exists)
 StepKernel march_kernel_f32(int nx, int nbuf, bool mass, int ty = 0);
+// the march kernels of ch_march2.cuh take the widths and tiles they cover
+bool march2_enabled();
 StepKernel march_kernel_f64(int nx, int nbuf, int ty = 0);
 // ring depth of 3-D jobs of march widths that share launches (batch, server)
 constexpr int kMarchBatchNbuf = 3;

@@ -22,6 +22,11 @@ def test_bounded_tma_wait_reports_error_and_context_survives(monkeypatch, oracle
             sim.sync(timeout_us=60_000_000)
         assert e.value.code == mb._lib.MG_EDEVICE
         assert sim.steps == 0  # the step did not complete
+        # copies may have been in flight when the kernel gave up: the handle
+        # refuses further steps instead of stepping untrusted state
+        with pytest.raises(mb.MGError) as e2:
+            sim.step(1)
+        assert e2.value.code == mb._lib.MG_EDEVICE
     monkeypatch.delenv("MG_FAULT_TX_EXTRA")
     monkeypatch.delenv("MG_SPIN_LIMIT")
     # same process, same device: a fresh handle works and is exact
