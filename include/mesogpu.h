@@ -324,6 +324,11 @@ typedef struct {
        (the launch lanes' device tables rewritten, the graphs kept) */
     double step_s, admit_s, retire_s;
     long long ticks, rebuilds, refreshes;
+    /* saturated rate: site-updates per second over the ticks that began
+       with jobs still queued (every slot or the HBM budget taken), and
+       how many ticks that was (0 when the queue never backed up) */
+    double sat_site_updates_per_s;
+    long long sat_ticks;
 } mg_server_stats;
 
 #define MG_JOB_QUEUED 0

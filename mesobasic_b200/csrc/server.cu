@@ -74,6 +74,10 @@ struct mg_server {
     double site_updates = 0;
     double step_s = 0, admit_s = 0, retire_s = 0;  // worker time (see mg_server_stats)
     long long ticks = 0;
+    // ticks that began with jobs still queued (every slot or the budget
+    // taken): their time and the site-updates they ran
+    double sat_s = 0, sat_updates = 0;
+    long long sat_ticks = 0;
 
     void run();
     void admit();
@@ -206,6 +210,17 @@ void mg_server::run()
         const long long k = steps_per_tick;
         // steps only when some admitted job still has steps to take
         const bool stepping = running.size() > finished.size();
+        // a tick that starts with a backlog runs at the server's saturated
+        // rate; the site-updates it runs are those its jobs still owe
+        bool backlog;
+        double tick_updates = 0;
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            backlog = !queue.empty();
+            for (ServerJob* sj : running)
+                tick_updates += (double)sj->p.nx * sj->p.ny * sj->p.nz *
+                                (double)std::min(k, std::max(0LL, sj->nsteps - sj->done_steps));
+        }
         const auto t0 = Clock::now();
         int rc = stepping ? eng.enqueue_steps((int)k) : MG_OK;
         const auto t1 = Clock::now();
@@ -217,8 +232,14 @@ void mg_server::run()
             std::lock_guard<std::mutex> lock(mu);
             retire_s += rs;
             if (stepping) {
-                step_s += seconds_since(t0);
+                const double ts = seconds_since(t0);
+                step_s += ts;
                 ++ticks;
+                if (backlog && rc == MG_OK) {
+                    sat_s += ts;
+                    sat_updates += tick_updates;
+                    ++sat_ticks;
+                }
             }
         }
         std::vector<ServerJob*> snapshot = running;
@@ -371,6 +392,8 @@ int mg_server_stats_get(mg_server_t* s, mg_server_stats* out)
             st.site_updates_per_s = s->site_updates / wall;
         }
     }
+    st.sat_ticks = s->sat_ticks;
+    st.sat_site_updates_per_s = s->sat_s > 0 ? s->sat_updates / s->sat_s : 0.0;
     st.hbm_in_use_gb = s->in_use / 1e9;
     st.hbm_peak_gb = s->peak / 1e9;
     *out = st;
