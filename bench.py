@@ -41,7 +41,8 @@ METRIC = "GLUPS & % HBM roofline (FP32 vs FP64)"
 # DRAM traffic per launch is read from the committed ncu summaries (one
 # capture of the same kernel and tiling), not measured inside this run
 TRAFFIC_SOURCE = {"fp64": "ncu capture in profiles/ncu_ch_march_fp64_256.md (same kernel and tiling)",
-                  "fp32": "ncu capture in profiles/ncu_ch_march_fp32_256.md (same kernel and tiling)"}
+                  "fp32": "ncu capture in profiles/ncu_ch_march2_fp32_256.md (same kernel and tiling)"}
+TRAFFIC_FILE = {"fp64": "ncu_ch_march_fp64_256.md", "fp32": "ncu_ch_march2_fp32_256.md"}
 
 
 def load_peaks():
@@ -55,7 +56,7 @@ def load_peaks():
 
 def load_traffic(dtype):
     """DRAM bytes per launch of the step kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", f"ncu_ch_march_{dtype}_256.md")
+    p = os.path.join(ROOT, "profiles", TRAFFIC_FILE[dtype])
     if not os.path.exists(p):
         return None
     for line in open(p):
