@@ -325,8 +325,9 @@ typedef struct {
     double step_s, admit_s, retire_s;
     long long ticks, rebuilds, refreshes;
     /* saturated rate: site-updates per second over the ticks that began
-       with jobs still queued (every slot or the HBM budget taken), and
-       how many ticks that was (0 when the queue never backed up) */
+       with jobs still queued (every slot or the HBM budget taken), each
+       timed from its start to the next tick's start, and how many ticks
+       that was (0 when the queue never backed up) */
     double sat_site_updates_per_s;
     long long sat_ticks;
 } mg_server_stats;

@@ -731,9 +731,13 @@ Engine::~Engine()
     cudaFree(d_diag_);
     cudaFreeHost(h_diag_);
     cudaFreeHost(h_state_);
+    if (admit_) cudaStreamSynchronize(admit_);
+    cudaFree(d_stage_adm_);
+    cudaFree(d_part_adm_);
     free_graveyard();
     for (cudaStream_t st : aux_) cudaStreamDestroy(st);
     if (side) cudaStreamDestroy(side);
+    if (admit_) cudaStreamDestroy(admit_);
     for (cudaEvent_t ev : aux_ev_) cudaEventDestroy(ev);
     if (fork_ev_) cudaEventDestroy(fork_ev_);
     if (stream) cudaStreamDestroy(stream);
@@ -768,7 +772,14 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const Fh
     j->noise_negate = noise_negate;
     if (fh && fh->model == kFhSips) j->noise_cutoff = fh->phiCutoff;
     MG_TRY(make_geometry(p, &j->g));
+    if (free_slots_.empty() && !released_slots_.empty() && !admitting_) {
+        // no launch in flight once the stream is idle: released slots are free
+        MG_CUDA(cudaStreamSynchronize(stream));
+        free_slots_.insert(free_slots_.end(), released_slots_.begin(), released_slots_.end());
+        released_slots_.clear();
+    }
     if (free_slots_.empty()) return fail(MG_ENOMEM, "no free job slot (capacity %d)", capacity_);
+    const cudaStream_t wst = work_stream();
     if (fh && (p.precision != MG_FP64 || p.mass_correct))
         return fail(MG_EINVAL, "the variable-mobility model runs in FP64 without mass feedback");
     MG_CUDA(cudaSetDevice(device));
@@ -801,7 +812,7 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const Fh
             FhDev f = *fh;
             f.mu = j->d_mu;
             f.mob = j->d_mob;
-            e = cudaMemcpyAsync(j->d_fh, &f, sizeof f, cudaMemcpyHostToDevice, stream);
+            e = cudaMemcpyAsync(j->d_fh, &f, sizeof f, cudaMemcpyHostToDevice, wst);
         }
     }
     if (e != cudaSuccess) {
@@ -820,7 +831,7 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const Fh
         CUtensorMap maps[4];
         int rc = encode_maps(*j, maps);
         if (rc == MG_OK) {
-            cudaError_t ce = cudaMemcpyAsync(j->d_tmap, maps, sizeof maps, cudaMemcpyHostToDevice, stream);
+            cudaError_t ce = cudaMemcpyAsync(j->d_tmap, maps, sizeof maps, cudaMemcpyHostToDevice, wst);
             if (ce != cudaSuccess) rc = fail(MG_ECUDA, "copying tensor maps: %s", cudaGetErrorString(ce));
         }
         if (rc != MG_OK) {
@@ -838,7 +849,7 @@ int Engine::add_job(const mg_ch_params& p, long long target, Job** out, const Fh
     free_slots_.pop_back();
     JobDev jd;
     fill_jobdev(*j, &jd);
-    MG_CUDA(cudaMemcpyAsync(d_jobs_ + j->slot, &jd, sizeof jd, cudaMemcpyHostToDevice, stream));
+    MG_CUDA(cudaMemcpyAsync(d_jobs_ + j->slot, &jd, sizeof jd, cudaMemcpyHostToDevice, wst));
     jobs.push_back(j.get());
     dirty_ = true;
     *out = j.release();
@@ -854,9 +865,27 @@ void Engine::remove_job(Job* j)
     // destruction: cudaFree waits for the whole device, once per call
     graveyard_.insert(graveyard_.end(), {j->buf[0], j->buf[1], (void*)j->d_tmap, (void*)j->d_partial, (void*)j->d_fh,
                                          (void*)j->d_mu, (void*)j->d_mob});
-    free_slots_.push_back(j->slot);
+    // a launch in flight may still name the slot (its items skip a finished
+    // job): free again after the next rebuild, which waits for the stream
+    released_slots_.push_back(j->slot);
     delete j;
     dirty_ = true;
+}
+
+int Engine::begin_admission()
+{
+    MG_CUDA(cudaSetDevice(device));
+    if (!admit_) MG_CUDA(cudaStreamCreateWithFlags(&admit_, cudaStreamNonBlocking));
+    if (!d_part_adm_) MG_CUDA(cudaMalloc(&d_part_adm_, sizeof(long long) * kDiagBlocks));
+    admitting_ = true;
+    return MG_OK;
+}
+
+int Engine::end_admission()
+{
+    admitting_ = false;
+    if (admit_) MG_CUDA(cudaStreamSynchronize(admit_));
+    return MG_OK;
 }
 
 int Engine::set_tiling(Job* j, const mg_tiling& t)
@@ -1027,7 +1056,10 @@ bool Engine::refresh_tables(std::vector<Group>& ng)
 int Engine::rebuild()
 {
     MG_CUDA(cudaStreamSynchronize(stream));
+    if (admit_) MG_CUDA(cudaStreamSynchronize(admit_));
     free_graveyard();
+    free_slots_.insert(free_slots_.end(), released_slots_.begin(), released_slots_.end());
+    released_slots_.clear();
     // Several jobs: one ring depth per class (3 planes for 3-D jobs of a
     // march width, 4 for other 3-D jobs, 8 for 2-D) so that each class steps
     // in one launch.  Only nbuf changes; the tile rows and z chunks, which
@@ -1397,20 +1429,37 @@ int Engine::upload(Job* j, const double* host, long long target)
 {
     if (!host) return fail(MG_EINVAL, "null field");
     MG_CUDA(cudaSetDevice(device));
+    const cudaStream_t wst = work_stream();
     if (j->g.es == 8) {
-        MG_CUDA(cudaMemcpyAsync(j->buf[0], host, j->g.n * 8, cudaMemcpyHostToDevice, stream));
+        MG_CUDA(cudaMemcpyAsync(j->buf[0], host, j->g.n * 8, cudaMemcpyHostToDevice, wst));
     } else {
-        MG_TRY(ensure_stage(j->g.n));
-        MG_CUDA(cudaMemcpyAsync(d_stage_, host, j->g.n * 8, cudaMemcpyHostToDevice, stream));
-        ch_convert<double, float><<<4 * info.sms, 256, 0, stream>>>(d_stage_, static_cast<float*>(j->buf[0]), j->g.n);
+        double* stage;
+        if (admitting_) {
+            // the admission's own staging: the engine's is in use by the
+            // downloads of finished jobs on the side stream
+            if (stage_adm_n_ < j->g.n) {
+                if (d_stage_adm_) graveyard_.push_back(d_stage_adm_);  // a copy may still read it
+                d_stage_adm_ = nullptr;
+                stage_adm_n_ = 0;
+                MG_CUDA(cudaMalloc(&d_stage_adm_, j->g.n * sizeof(double)));
+                stage_adm_n_ = j->g.n;
+            }
+            stage = d_stage_adm_;
+        } else {
+            MG_TRY(ensure_stage(j->g.n));
+            stage = d_stage_;
+        }
+        MG_CUDA(cudaMemcpyAsync(stage, host, j->g.n * 8, cudaMemcpyHostToDevice, wst));
+        ch_convert<double, float><<<4 * info.sms, 256, 0, wst>>>(stage, static_cast<float*>(j->buf[0]), j->g.n);
     }
     j->target = target;
-    ch_job_reset<<<1, 32, 0, stream>>>(d_jobs_ + j->slot, target < 0 ? LLONG_MAX : target);
+    ch_job_reset<<<1, 32, 0, wst>>>(d_jobs_ + j->slot, target < 0 ? LLONG_MAX : target);
     if (j->g.es == 4) {
-        // d_diag_part_ (3 x kDiagBlocks double2) is scratch for the block sums
-        long long* part = reinterpret_cast<long long*>(d_diag_part_);
-        ch_mass_partial<<<kDiagBlocks, kDiagThreads, 0, stream>>>(d_jobs_ + j->slot, part);
-        ch_mass_final<<<1, 32, 0, stream>>>(part, kDiagBlocks, d_jobs_ + j->slot);
+        // scratch for the block sums: d_diag_part_ (3 x kDiagBlocks double2),
+        // or the admission's own
+        long long* part = admitting_ ? d_part_adm_ : reinterpret_cast<long long*>(d_diag_part_);
+        ch_mass_partial<<<kDiagBlocks, kDiagThreads, 0, wst>>>(d_jobs_ + j->slot, part);
+        ch_mass_final<<<1, 32, 0, wst>>>(part, kDiagBlocks, d_jobs_ + j->slot);
     }
     MG_CUDA(cudaGetLastError());
     return MG_OK;

@@ -112,6 +112,15 @@ class Engine {
     int set_tiling(Job* j, const mg_tiling& t);
 
     int upload(Job* j, const double* host, long long target);  // resets step
+    // Admission beside running steps: between begin_admission and
+    // end_admission, add_job and upload issue their device work on a stream
+    // of their own with staging buffers of their own, so they overlap the
+    // steps in flight on `stream` (the new jobs join the launches at the next
+    // enqueue_steps).  end_admission waits for that work.  Slots of removed
+    // jobs are reused only after the next rebuild, when no launch in flight
+    // still names them.
+    int begin_admission();
+    int end_admission();
     int download(Job* j, double* host);                         // syncs
     int diagnostics(Job* j, mg_ch_stats* out);                  // syncs
     // The same for a job that has reached its step target, on a side stream
@@ -208,6 +217,13 @@ class Engine {
     int* d_err_ = nullptr;
     bool poisoned_ = false;  // a kernel reported a device error: no further steps
     std::vector<int> free_slots_;
+    std::vector<int> released_slots_;  // slots of removed jobs, free again after the next rebuild
+    bool admitting_ = false;
+    cudaStream_t admit_ = nullptr;      // admission stream (begin_admission)
+    double* d_stage_adm_ = nullptr;     // admission staging (doubles) and mass partials
+    size_t stage_adm_n_ = 0;
+    long long* d_part_adm_ = nullptr;
+    cudaStream_t work_stream() const { return admitting_ ? admit_ : stream; }
     std::vector<Group> groups_;
     bool dirty_ = true;
     std::map<int, cudaGraphExec_t> graphs_;

@@ -80,7 +80,9 @@ struct mg_server {
     long long sat_ticks = 0;
 
     void run();
-    void admit();
+    // jobs admitted beside a running tick, joining at the next one
+    std::vector<ServerJob*> arrived;
+    void admit(bool beside_tick);
     void retire(ServerJob* sj, bool ok, const char* why);
 };
 
@@ -95,14 +97,16 @@ static size_t job_bytes(const mg_ch_params& p)
 // (their bytes counted, taken off the queue).  The device work -- buffers,
 // tensor maps, upload of the initial field -- runs after the lock is
 // released: only the worker thread touches the engine, so submitters never
-// wait for an allocation or a copy.
-void mg_server::admit()
+// wait for an allocation or a copy.  beside_tick: the worker has a tick in
+// flight; the device work goes on the engine's admission stream, overlapping
+// it, and the jobs join the tick after (`arrived`).
+void mg_server::admit(bool beside_tick)
 {
     std::vector<ServerJob*> take;
     {
         std::lock_guard<std::mutex> lock(mu);
         for (auto it = queue.begin(); it != queue.end();) {
-            if ((int)(running.size() + take.size()) >= max_inflight) break;
+            if ((int)(running.size() + arrived.size() + take.size()) >= max_inflight) break;
             ServerJob* sj = *it;
             if ((double)(in_use + sj->bytes) > budget) {
                 ++it;
@@ -117,6 +121,7 @@ void mg_server::admit()
     if (take.empty()) return;
     std::vector<ServerJob*> ok, bad;
     std::vector<std::string> why;
+    if (beside_tick && eng.begin_admission() != MG_OK) beside_tick = false;
     for (ServerJob* sj : take) {
         mg::Job* j = nullptr;
         int rc = eng.add_job(sj->p, sj->nsteps, &j);
@@ -127,14 +132,24 @@ void mg_server::admit()
             why.push_back(mg::last_error());
             continue;
         }
-        std::vector<double>().swap(sj->ic);
         sj->job = j;
         ok.push_back(sj);
     }
+    if (beside_tick && eng.end_admission() != MG_OK) {
+        // the uploads did not complete: the jobs fail
+        for (ServerJob* sj : ok) {
+            eng.remove_job(sj->job);
+            sj->job = nullptr;
+            bad.push_back(sj);
+            why.push_back(mg::last_error());
+        }
+        ok.clear();
+    }
+    for (ServerJob* sj : ok) std::vector<double>().swap(sj->ic);  // the uploads have read it
     std::lock_guard<std::mutex> lock(mu);
     for (ServerJob* sj : ok) {
         sj->state = MG_JOB_RUNNING;
-        running.push_back(sj);
+        (beside_tick ? arrived : running).push_back(sj);
     }
     for (size_t i = 0; i < bad.size(); ++i) {
         ServerJob* sj = bad[i];
@@ -196,10 +211,15 @@ void mg_server::run()
     // jobs that reached their step count in the last tick: retired (field
     // and diagnostics read on a side stream) while the next tick runs
     std::vector<ServerJob*> finished;
+    // the saturated rate counts whole iterations, from one tick's start to
+    // the next one's (the admissions and retirements between them included)
+    bool prev_sat = false;
+    double prev_updates = 0;
+    Clock::time_point prev_t0;
     for (;;) {
         for (;;) {
             auto t0 = Clock::now();
-            admit();
+            admit(false);
             const double as = seconds_since(t0);
             std::unique_lock<std::mutex> lock(mu);
             admit_s += as;
@@ -222,37 +242,56 @@ void mg_server::run()
                                 (double)std::min(k, std::max(0LL, sj->nsteps - sj->done_steps));
         }
         const auto t0 = Clock::now();
+        if (prev_sat) {
+            std::lock_guard<std::mutex> lock(mu);
+            sat_s += std::chrono::duration<double>(t0 - prev_t0).count();
+            sat_updates += prev_updates;
+            ++sat_ticks;
+        }
+        prev_sat = false;
         int rc = stepping ? eng.enqueue_steps((int)k) : MG_OK;
         const auto t1 = Clock::now();
         for (ServerJob* sj : finished) retire(sj, true, nullptr);
         finished.clear();
         const double rs = seconds_since(t1);
+        // admit the next tick's jobs while this one runs
+        const auto t2 = Clock::now();
+        if (stepping && rc == MG_OK) admit(true);
+        const double as2 = seconds_since(t2);
         if (stepping && rc == MG_OK) rc = eng.sync(600LL * 1000 * 1000);
         {
             std::lock_guard<std::mutex> lock(mu);
             retire_s += rs;
+            admit_s += as2;
             if (stepping) {
                 const double ts = seconds_since(t0);
                 step_s += ts;
                 ++ticks;
                 if (backlog && rc == MG_OK) {
-                    sat_s += ts;
-                    sat_updates += tick_updates;
-                    ++sat_ticks;
+                    prev_sat = true;
+                    prev_updates = tick_updates;
+                    prev_t0 = t0;
                 }
             }
         }
-        std::vector<ServerJob*> snapshot = running;
+        std::vector<ServerJob*> snapshot = running;  // the jobs of this tick
+        {
+            // the jobs admitted beside this tick join the next one
+            std::lock_guard<std::mutex> lock(mu);
+            running.insert(running.end(), arrived.begin(), arrived.end());
+            arrived.clear();
+        }
         if (rc != MG_OK) {
             const std::string why = mg::last_error();
-            for (ServerJob* sj : snapshot) retire(sj, false, why.c_str());
+            const std::vector<ServerJob*> all = running;
+            for (ServerJob* sj : all) retire(sj, false, why.c_str());
             continue;
         }
-        if (!stepping) continue;
-        for (ServerJob* sj : snapshot) {
-            sj->done_steps = std::min(sj->nsteps, sj->done_steps + k);
-            if (sj->done_steps >= sj->nsteps) finished.push_back(sj);
-        }
+        if (stepping)
+            for (ServerJob* sj : snapshot) {
+                sj->done_steps = std::min(sj->nsteps, sj->done_steps + k);
+                if (sj->done_steps >= sj->nsteps) finished.push_back(sj);
+            }
     }
 }
 
@@ -266,7 +305,9 @@ int mg_server_create(int device, double hbm_budget_gb, int max_jobs_in_flight, i
     *out = nullptr;
     std::unique_ptr<mg_server> s(new (std::nothrow) mg_server);
     if (!s) return fail(MG_ENOMEM, "host allocation failed");
-    MG_TRY(s->eng.init(device, max_jobs_in_flight));
+    // twice the slots of the jobs in flight: a retired job's slot is reused
+    // only after the next rebuild, while admissions run beside a tick
+    MG_TRY(s->eng.init(device, 2 * max_jobs_in_flight));
     s->eng.batch_tiling = true;
     // tile target of the served jobs: 320 threads a CTA and 64-plane z
     // chunks took 11 % less GPU time on the served stream than 256 / 16
