@@ -622,9 +622,18 @@ __global__ void ch_noise_kernel(JobDev* job)
 //    the constant Mpp (Mnn): the fields step independently.  The GPU takes
 //    the same arithmetic.
 
-__device__ __forceinline__ size_t fh_at(int x, int y, int z, const JobDev& J)
+// The neighbours of site s one step down / up an axis of length n and
+// stride st, from its coordinate i: the periodic wrap, or on a no-flux axis
+// the site itself (the ghost copy): the site at coordinate
+// wrap_or_clamp(i -/+ 1, n) on that axis, without its modulo and without
+// forming the index from (x, y, z).
+__device__ __forceinline__ size_t fh_down(size_t s, int i, size_t st, size_t span, bool per)
 {
-    return ((size_t)z * J.ny + y) * J.nx + x;
+    return i > 0 ? s - st : (per ? s + span : s);
+}
+__device__ __forceinline__ size_t fh_up(size_t s, int i, int n, size_t st, size_t span, bool per)
+{
+    return i < n - 1 ? s + st : (per ? s - span : s);
 }
 
 // Pass 1: mu and the reciprocal mobility 1/mob of every site (F.mu, F.mob).
@@ -651,15 +660,18 @@ __global__ void fh_mu_mob_kernel(JobDev* job)
     const size_t r0 = first / nx, dr = stride / nx;
     int y = (int)(r0 % ny), z = (int)(r0 / ny);
     const int dy = (int)(dr % ny), dz = (int)(dr / ny);
+    // strides and wrap spans of the three axes
+    const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+    const size_t wx = (size_t)(nx - 1), wy = (size_t)(ny - 1) * sy, wz = (size_t)(nz - 1) * sz;
     for (size_t s = first; s < n; s += stride) {
         const double cc = c[s];
-        const double xp = c[fh_at(wrap_or_clamp(x + 1, nx, pX), y, z, J)], xm = c[fh_at(wrap_or_clamp(x - 1, nx, pX), y, z, J)];
-        const double zp = c[fh_at(x, y, wrap_or_clamp(z + 1, nz, pZ), J)], zm = c[fh_at(x, y, wrap_or_clamp(z - 1, nz, pZ), J)];
+        const double xp = c[fh_up(s, x, nx, 1, wx, pX)], xm = c[fh_down(s, x, 1, wx, pX)];
+        const double zp = c[fh_up(s, z, nz, sz, wz, pZ)], zm = c[fh_down(s, z, sz, wz, pZ)];
         double lapc;
         if (J.flags & JF_FLAT) {
             lapc = A::add(axis_term(xp, xm, cc, J.cx, J.flags & JF_DIV_X), axis_term(zp, zm, cc, J.cz, J.flags & JF_DIV_Z));
         } else {
-            const double yp = c[fh_at(x, wrap_or_clamp(y + 1, ny, pY), z, J)], ym = c[fh_at(x, wrap_or_clamp(y - 1, ny, pY), z, J)];
+            const double yp = c[fh_up(s, y, ny, sy, wy, pY)], ym = c[fh_down(s, y, sy, wy, pY)];
             lapc = A::add(A::add(axis_term(xp, xm, cc, J.cx, J.flags & JF_DIV_X), axis_term(yp, ym, cc, J.cy, J.flags & JF_DIV_Y)),
                           axis_term(zp, zm, cc, J.cz, J.flags & JF_DIV_Z));
         }
@@ -691,15 +703,17 @@ __device__ __forceinline__ double fh_update_site(const JobDev& J, const double* 
     const int nx = J.nx, ny = J.ny, nz = J.nz;
     const bool pX = J.flags & JF_PER_X, pY = J.flags & JF_PER_Y, pZ = J.flags & JF_PER_Z;
     const double a0 = mu[s], ro = rmob[s];
-    const size_t ixm = fh_at(wrap_or_clamp(x - 1, nx, pX), y, z, J), ixp = fh_at(wrap_or_clamp(x + 1, nx, pX), y, z, J);
-    const size_t izm = fh_at(x, y, wrap_or_clamp(z - 1, nz, pZ), J), izp = fh_at(x, y, wrap_or_clamp(z + 1, nz, pZ), J);
+    const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+    const size_t wx = (size_t)(nx - 1), wy = (size_t)(ny - 1) * sy, wz = (size_t)(nz - 1) * sz;
+    const size_t ixm = fh_down(s, x, 1, wx, pX), ixp = fh_up(s, x, nx, 1, wx, pX);
+    const size_t izm = fh_down(s, z, sz, wz, pZ), izp = fh_up(s, z, nz, sz, wz, pZ);
     const double lx = fh_axis_r(mu[ixm], mu[ixp], a0, rmob[ixm], rmob[ixp], ro, J.cx, J.flags & JF_DIV_X);
     const double lz = fh_axis_r(mu[izm], mu[izp], a0, rmob[izm], rmob[izp], ro, J.cz, J.flags & JF_DIV_Z);
     double lap;
     if (J.flags & JF_FLAT) {
         lap = A::add(lx, lz);
     } else {
-        const size_t iym = fh_at(x, wrap_or_clamp(y - 1, ny, pY), z, J), iyp = fh_at(x, wrap_or_clamp(y + 1, ny, pY), z, J);
+        const size_t iym = fh_down(s, y, sy, wy, pY), iyp = fh_up(s, y, ny, sy, wy, pY);
         const double ly = fh_axis_r(mu[iym], mu[iyp], a0, rmob[iym], rmob[iyp], ro, J.cy, J.flags & JF_DIV_Y);
         lap = A::add(A::add(lx, ly), lz);
     }
