@@ -1030,6 +1030,8 @@ bool Engine::refresh_tables(std::vector<Group>& ng)
             const Group& L = groups_[l];
             if (used[l] || L.key != g.key || L.sub != g.sub || group_kernel(L) != group_kernel(g)) continue;
             if (g.block > L.block || g.cplane > L.cplane || g.mplane > L.mplane) return false;
+            // more items than CTAs, while the lane could keep more resident
+            if (g.nitems > L.grid && L.grid < L.grid_max) return false;
             lane_of[i] = (int)l;
             used[l] = true;
             break;
@@ -1175,6 +1177,7 @@ int Engine::rebuild()
             h.block = std::max(h.block, g.block);
             h.cplane = std::max(h.cplane, g.cplane);
             h.mplane = std::max(h.mplane, g.mplane);
+            h.items = std::max(h.items, g.nitems);
             g.block = h.block;
             g.cplane = h.cplane;
             g.mplane = h.mplane;
@@ -1184,8 +1187,14 @@ int Engine::rebuild()
         int occ = 1;
         MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, group_kernel(g), g.block, g.smem));
         occ = std::max(occ, 1);
-        // a stable lane keeps its grid whatever the item count: persistent CTAs
-        g.grid = stable_lanes ? info.sms * occ : std::min(g.nitems, info.sms * occ);
+        // a stable lane keeps its grid whatever the item count: persistent
+        // CTAs, as many as the most items the lane has held (up to what the
+        // GPU keeps resident), so that a lane of a few small jobs does not
+        // launch a full grid of CTAs that find no item every step; a job set
+        // with more items than the grid rebuilds the lane (refresh_tables)
+        g.grid_max = info.sms * occ;
+        g.grid = stable_lanes ? std::min(g.grid_max, std::max(1, hw_[{g.key, g.sub}].items))
+                              : std::min(g.nitems, g.grid_max);
         g.table_cap = stable_lanes ? std::max(capacity_, 1) : (int)g.jobs.size();
         MG_CUDA(cudaMalloc(&g.d_item_begin, sizeof(int) * (g.table_cap + 1)));
         MG_CUDA(cudaMalloc(&g.d_slot, sizeof(int) * g.table_cap));

@@ -178,6 +178,7 @@ class Engine {
         int nbuf = 4;
         std::vector<Job*> jobs;
         int nitems = 0, grid = 0, block = 0;
+        int grid_max = 0;  // SMs x occupancy: the most CTAs a launch of the lane can keep resident
         int fixed_nx = 0;  // row width shared by every job of the group (0: mixed)
         int fixed_ty = 0;  // tile height shared by every job of the group (0: mixed)
         size_t smem = 0;
@@ -191,6 +192,7 @@ class Engine {
     StepKernel group_kernel(const Group& g) const;
     struct HighWater {
         int block = 0, cplane = 0, mplane = 0;
+        int items = 0;  // most work items the lane has held
     };
     std::map<std::pair<long long, int>, HighWater> hw_;  // stable lanes: largest tile seen per class
     long long refreshes_ = 0;
