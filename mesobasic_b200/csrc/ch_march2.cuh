@@ -1,5 +1,5 @@
-// The FP32 march step (periodic 3-D, equal spacing, power-of-two row width
-// NXC <= 256) written for the compiler's scheduler:
+// The FP32 march step (periodic 3-D, equal spacing, row width NXC a multiple
+// of 32 up to 256) written for the compiler's scheduler:
 //  - shared memory is read and written through C++ float4 accesses, which
 //    the compiler may order freely between the ring waits and the barriers
 //    (the TMA ring and its mbarriers stay in PTX);
@@ -87,7 +87,10 @@ template <int NXC, int NBUF, bool MASS, int TY>
 __device__ __forceinline__ bool march2_item(const StepArgs& a, JobDev* J, int local, MarchCta& cta)
 {
     constexpr int NQ = NXC / 8;  // threads per row
-    static_assert(NXC <= 256 && NXC % 64 == 0 && (NQ & (NQ - 1)) == 0, "power-of-two rows of at most 256");
+    // rows whose threads form a power-of-two segment of a warp take their
+    // x-neighbours from shuffles, other rows from the row in shared memory
+    constexpr bool SEG = NQ <= 32 && (NQ & (NQ - 1)) == 0;
+    static_assert(NXC >= 64 && NXC <= 256 && NXC % 32 == 0, "rows of 64..256 sites, a multiple of 32");
     static_assert(TY >= 0 && NBUF >= 3 && NBUF <= 8, "tile height, ring depth");
     constexpr uint32_t ROWB = NXC * 4;
     constexpr int U = (NBUF % 3 == 0) ? NBUF : 3 * NBUF;  // planes per unrolled block
@@ -106,6 +109,8 @@ __device__ __forceinline__ bool march2_item(const StepArgs& a, JobDev* J, int lo
     const int rsrc = segbase | ((lane + 1) & (NQ - 1));
     const bool first = tx == 0, last = tx == NQ - 1;
     const int xA = tx * 4;
+    // row-relative offsets of the four x-neighbours (shared-memory edges)
+    const int oLA = (xA + NXC - 1) % NXC, oRA = xA + 4, oLB = xA + NXC / 2 - 1, oRB = (xA + NXC / 2 + 4) % NXC;
 
     // the per-item scalars that need 64-bit divisions are formed once, by
     // thread 0, and broadcast (head->red is free until the item epilogue)
@@ -177,7 +182,9 @@ __device__ __forceinline__ bool march2_item(const StepArgs& a, JobDev* J, int lo
     const bool active = tid < NQ * MY;
     const int m = active ? tid / NQ : 0;
     const float* const cOwn = cring + (m + 1) * NXC + xA;
+    const float* const cRow = cring + (m + 1) * NXC;
     float* const mOwn = mring + m * NXC + xA;
+    const float* const mRow = mring + m * NXC;
     const float* const mUp = mring + max(m - 1, 0) * NXC + xA;
     const float* const mDn = mring + min(m + 1, MY - 1) * NXC + xA;
     const int y = y0 - 1 + m;
@@ -220,14 +227,22 @@ __device__ __forceinline__ bool march2_item(const StepArgs& a, JobDev* J, int lo
         ph ^= 1u << s;
         ++nw;
     };
-    // x-neighbours of a strip's two halves from the lanes of its row segment
-    auto edges = [&](const S8& v, float& lA, float& rA, float& lB, float& rB) {
-        const float sAL = __shfl_sync(0xffffffffu, v.a.w, lsrc), sBL = __shfl_sync(0xffffffffu, v.b.w, lsrc);
-        const float sAF = __shfl_sync(0xffffffffu, v.a.x, rsrc), sBF = __shfl_sync(0xffffffffu, v.b.x, rsrc);
-        lA = first ? sBL : sAL;
-        lB = first ? sAL : sBL;
-        rA = last ? sBF : sAF;
-        rB = last ? sAF : sBF;
+    // x-neighbours of a strip's two halves: from the lanes of its row
+    // segment, or from its row in shared memory
+    auto edges = [&](const S8& v, const float* row, float& lA, float& rA, float& lB, float& rB) {
+        if constexpr (SEG) {
+            const float sAL = __shfl_sync(0xffffffffu, v.a.w, lsrc), sBL = __shfl_sync(0xffffffffu, v.b.w, lsrc);
+            const float sAF = __shfl_sync(0xffffffffu, v.a.x, rsrc), sBF = __shfl_sync(0xffffffffu, v.b.x, rsrc);
+            lA = first ? sBL : sAL;
+            lB = first ? sAL : sBL;
+            rA = last ? sBF : sAF;
+            rB = last ? sAF : sBF;
+        } else {
+            lA = row[oLA];
+            rA = row[oRA];
+            lB = row[oLB];
+            rB = row[oRB];
+        }
     };
 
     S8 R[3], Mq[3];
@@ -265,7 +280,7 @@ __device__ __forceinline__ bool march2_item(const StepArgs& a, JobDev* J, int lo
                 const S8 up = lds8<NXC>(pl - NXC);
                 const S8 dn = lds8<NXC>(pl + NXC);
                 float lA, rA, lB, rB;
-                edges(cc, lA, rA, lB, rB);
+                edges(cc, cRow + sI * CPL, lA, rA, lB, rB);
                 float2 lp[4];
                 lap8(cc, lA, rA, lB, rB, up, dn, cp, cn, lp);
                 const float2 c2[4] = {lo2(cc.a), hi2(cc.a), lo2(cc.b), hi2(cc.b)};
@@ -290,7 +305,7 @@ __device__ __forceinline__ bool march2_item(const StepArgs& a, JobDev* J, int lo
                 const S8 up = lds8<NXC>(mUp + mslp * MPL);
                 const S8 dn = lds8<NXC>(mDn + mslp * MPL);
                 float lA, rA, lB, rB;
-                edges(mc, lA, rA, lB, rB);
+                edges(mc, mRow + mslp * MPL, lA, rA, lB, rB);
                 if (outrow) {
                     float2 lp[4];
                     lap8(mc, lA, rA, lB, rB, up, dn, mp, mn, lp);

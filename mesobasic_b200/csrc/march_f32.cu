@@ -36,8 +36,8 @@ static StepKernel march_f32_width(int nx, int nbuf)
 }
 
 // The FP32 march kernels of ch_march2.cuh (C++ shared-memory accesses and
-// float2 f32x2 builtins; measured 1-4 % faster, bit-identical) take the
-// power-of-two widths at ring depth 3; MG_MARCH2=0 keeps ch_march_kernel.
+// float2 f32x2 builtins; measured 1-4 % faster, bit-identical) take every
+// march width at ring depth 3; MG_MARCH2=0 keeps ch_march_kernel.
 bool march2_enabled()
 {
     static const bool v = [] {
@@ -58,7 +58,11 @@ StepKernel march_kernel_f32(int nx, int nbuf, bool mass, int ty)
     if (march2_enabled() && nbuf == 3) {
         switch (nx) {
         case 64: return mass ? ch_march2_kernel<64, 3, true, 0> : ch_march2_kernel<64, 3, false, 0>;
+        case 96: return mass ? ch_march2_kernel<96, 3, true, 0> : ch_march2_kernel<96, 3, false, 0>;
         case 128: return mass ? ch_march2_kernel<128, 3, true, 0> : ch_march2_kernel<128, 3, false, 0>;
+        case 160: return mass ? ch_march2_kernel<160, 3, true, 0> : ch_march2_kernel<160, 3, false, 0>;
+        case 192: return mass ? ch_march2_kernel<192, 3, true, 0> : ch_march2_kernel<192, 3, false, 0>;
+        case 224: return mass ? ch_march2_kernel<224, 3, true, 0> : ch_march2_kernel<224, 3, false, 0>;
         case 256: return mass ? ch_march2_kernel<256, 3, true, 0> : ch_march2_kernel<256, 3, false, 0>;
         default: break;
         }
