@@ -391,9 +391,10 @@ __device__ __forceinline__ bool march2_item(const StepArgs& a, JobDev* J, int lo
 }
 
 // Every job of the launch: FP32, row width NXC, tile height TY (0: each job's own).
-// A fixed tile height bounds the registers for two CTAs per SM.
+// A fixed tile height bounds the registers for two CTAs per SM (of the
+// block the host launches: the tile's threads rounded up to whole warps).
 template <int NXC, int NBUF, bool MASS, int TY>
-__global__ void __launch_bounds__(TY > 0 ? (TY + 2) * (NXC / 8) : kMaxBlock, TY > 0 ? 2 : 1)
+__global__ void __launch_bounds__(TY > 0 ? ((TY + 2) * (NXC / 8) + 31) / 32 * 32 : kMaxBlock, TY > 0 ? 2 : 1)
     ch_march2_kernel(StepArgs a)
 {
     step_counts(a);

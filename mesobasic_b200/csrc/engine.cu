@@ -430,6 +430,9 @@ int prepare_kernels(const DevInfo& d)
     for (int ms = 0; ms < 2; ++ms)
         MG_CUDA(cudaFuncSetAttribute(march_kernel_f32(256, 3, ms, 8), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)d.smem_optin));
+    for (const auto& wt : {std::pair<int, int>{64, 32}, {96, 24}, {128, 16}, {160, 14}, {192, 11}})
+        MG_CUDA(cudaFuncSetAttribute(march_kernel_f32(wt.first, 3, true, wt.second),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d.smem_optin));
     for (int nb : {3, 6})
         MG_CUDA(cudaFuncSetAttribute(march_kernel_f64(256, nb, 7), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)d.smem_optin));

@@ -56,6 +56,15 @@ StepKernel march_kernel_f32(int nx, int nbuf, bool mass, int ty)
         return mass ? ch_march_kernel<float, 256, 3, true, 8> : ch_march_kernel<float, 256, 3, false, 8>;
     }
     if (march2_enabled() && nbuf == 3) {
+        // the tiles a batch of cubes 64..192 gets at its default targets
+        // (CTAs of ~320 threads, batch_tiling_for), specialised
+        if (mass) {
+            if (nx == 64 && ty == 32) return ch_march2_kernel<64, 3, true, 32>;
+            if (nx == 96 && ty == 24) return ch_march2_kernel<96, 3, true, 24>;
+            if (nx == 128 && ty == 16) return ch_march2_kernel<128, 3, true, 16>;
+            if (nx == 160 && ty == 14) return ch_march2_kernel<160, 3, true, 14>;
+            if (nx == 192 && ty == 11) return ch_march2_kernel<192, 3, true, 11>;
+        }
         switch (nx) {
         case 64: return mass ? ch_march2_kernel<64, 3, true, 0> : ch_march2_kernel<64, 3, false, 0>;
         case 96: return mass ? ch_march2_kernel<96, 3, true, 0> : ch_march2_kernel<96, 3, false, 0>;
