@@ -427,6 +427,7 @@ def run_serve(mb, dev, window_s, seed=11, rate=20.0, burst=0, torch=None, slots=
             "ticks": st["ticks"], "rebuilds": st["rebuilds"], "refreshes": st["refreshes"],
             "glups": st["site_updates_per_s"] / 1e9, "hbm_peak_gb": st["hbm_peak_gb"], "wall_s": wall,
             "sat_glups": st["sat_site_updates_per_s"] / 1e9, "sat_ticks": st["sat_ticks"], "slots": slots,
+            "gpu_busy": st["gpu_s"] / wall if wall > 0 else None,
             "submitted": len(arrivals), "batch_same_mix": same_mix, "submit_s": submit_s,
             "workload": (f"{burst} jobs submitted at once into {slots} slots (seed {seed})" if burst else
                          f"Poisson arrivals {rate:g}/s for {window_s:g} s (seed {seed})") + ": 50% 2-D edge "
@@ -546,7 +547,7 @@ def run_ours(args, rank, world, local_rank):
             # so that the queue holds jobs for most of the run
             sat = run_serve(mb, dev, args.serve_seconds, burst=args.serve_burst, torch=torch,
                             slots=args.serve_slots)
-            serve["saturated"] = {k: sat[k] for k in ("glups", "sat_glups", "sat_ticks", "slots", "sims_per_hour",
+            serve["saturated"] = {k: sat[k] for k in ("glups", "sat_glups", "sat_ticks", "slots", "gpu_busy", "sims_per_hour",
                                                       "p50_ms", "p99_ms", "completed", "ticks", "rebuilds",
                                                       "refreshes", "wall_s", "submit_s")}
             serve["saturated_worker_s"] = sat["worker_s"]

@@ -330,6 +330,9 @@ typedef struct {
        that was (0 when the queue never backed up) */
     double sat_site_updates_per_s;
     long long sat_ticks;
+    /* device time of the ticks (CUDA events around each tick's steps on the
+       engine's stream): against the wall time, how long the GPU worked */
+    double gpu_s;
 } mg_server_stats;
 
 #define MG_JOB_QUEUED 0

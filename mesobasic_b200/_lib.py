@@ -84,7 +84,8 @@ class ServerStats(ctypes.Structure):
                 ("hbm_in_use_gb", ctypes.c_double), ("hbm_peak_gb", ctypes.c_double),
                 ("step_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("retire_s", ctypes.c_double),
                 ("ticks", ctypes.c_longlong), ("rebuilds", ctypes.c_longlong), ("refreshes", ctypes.c_longlong),
-                ("sat_site_updates_per_s", ctypes.c_double), ("sat_ticks", ctypes.c_longlong)]
+                ("sat_site_updates_per_s", ctypes.c_double), ("sat_ticks", ctypes.c_longlong),
+                ("gpu_s", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -78,6 +78,8 @@ struct mg_server {
     // taken): their time and the site-updates they ran
     double sat_s = 0, sat_updates = 0;
     long long sat_ticks = 0;
+    double gpu_s = 0;  // device time of the ticks' steps (events on the engine stream)
+    cudaEvent_t ev_tick[2] = {nullptr, nullptr};
 
     void run();
     // jobs admitted beside a running tick, joining at the next one
@@ -249,7 +251,13 @@ void mg_server::run()
             ++sat_ticks;
         }
         prev_sat = false;
+        if (stepping && !ev_tick[0]) {
+            cudaEventCreate(&ev_tick[0]);
+            cudaEventCreate(&ev_tick[1]);
+        }
+        if (stepping && ev_tick[0]) cudaEventRecord(ev_tick[0], eng.stream);
         int rc = stepping ? eng.enqueue_steps((int)k) : MG_OK;
+        if (stepping && ev_tick[1]) cudaEventRecord(ev_tick[1], eng.stream);
         const auto t1 = Clock::now();
         for (ServerJob* sj : finished) retire(sj, true, nullptr);
         finished.clear();
@@ -267,6 +275,11 @@ void mg_server::run()
                 const double ts = seconds_since(t0);
                 step_s += ts;
                 ++ticks;
+                float ms = 0.f;
+                if (rc == MG_OK && ev_tick[1] && cudaEventElapsedTime(&ms, ev_tick[0], ev_tick[1]) == cudaSuccess)
+                    gpu_s += ms * 1e-3;
+                else
+                    cudaGetLastError();
                 if (backlog && rc == MG_OK) {
                     prev_sat = true;
                     prev_updates = tick_updates;
@@ -434,6 +447,7 @@ int mg_server_stats_get(mg_server_t* s, mg_server_stats* out)
         }
     }
     st.sat_ticks = s->sat_ticks;
+    st.gpu_s = s->gpu_s;
     st.sat_site_updates_per_s = s->sat_s > 0 ? s->sat_updates / s->sat_s : 0.0;
     st.hbm_in_use_gb = s->in_use / 1e9;
     st.hbm_peak_gb = s->peak / 1e9;
@@ -450,6 +464,8 @@ void mg_server_destroy(mg_server_t* s)
         s->cv_work.notify_all();
     }
     if (s->worker.joinable()) s->worker.join();
+    for (cudaEvent_t ev : s->ev_tick)
+        if (ev) cudaEventDestroy(ev);
     delete s;
 }
 
