@@ -148,6 +148,30 @@ def test_server_absorbs_job_set_changes_without_recapture():
         srv.close()
 
 
+def test_server_with_few_slots_recycles_them_and_keeps_results():
+    """More jobs than slots, submitted at once: jobs wait in the queue, each
+    tick admits the next ones beside the running steps, and a retired job's
+    slot is reused only after the next rebuild.  Every result is still
+    bit-identical to its standalone run, and the saturated rate and the
+    device time of the ticks are reported."""
+    jobs = job_set(seed=23, n=10)
+    steps = [30 + 11 * i for i in range(len(jobs))]
+    srv = mb.Server(hbm_budget_gb=4.0, max_jobs=3, steps_per_tick=20)
+    try:
+        ids = [srv.submit(p, ic, n) for (p, ic), n in zip(jobs, steps)]
+        for (p, ic), n, jid in zip(jobs, steps, ids):
+            got, st = srv.result(jid, p, timeout_us=120_000_000)
+            want, _ = alone(p, ic, n)
+            assert np.array_equal(got, want), jid
+            assert st["step"] == n
+        s = srv.stats()
+        assert s["completed"] == len(jobs) and s["failed"] == 0
+        assert s["sat_ticks"] > 0 and s["sat_site_updates_per_s"] > 0
+        assert 0 < s["gpu_s"] <= s["step_s"] + 1e-3
+    finally:
+        srv.close()
+
+
 def test_server_admission_respects_budget():
     # budget fits two 128^3 FP64 jobs (2 x 2 x 16.8 MB) but not three
     p = mb.make_params(128, 128, 128, 0.005)
