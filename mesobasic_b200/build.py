@@ -30,7 +30,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["engine.cu", "march_f32.cu", "march_f64.cu", "capi.cu", "server.cu", "noalloc.cu", "vtk_device.cu"]
 CPP_SOURCES = ["host_io.cpp"]
-HEADERS = ["ch_device.cuh", "ch_kernels.cuh", "ch_lean.cuh", "ch_march.cuh", "ch_march2.cuh", "ch_types.h", "mg_device.cuh", "engine.h"]
+HEADERS = ["ch_device.cuh", "ch_kernels.cuh", "ch_lean.cuh", "ch_march.cuh", "ch_march2.cuh", "fh_march.cuh", "ch_types.h", "mg_device.cuh", "engine.h"]
 DRIVER_SOURCES = ["input_file.cpp", "pf_model.cpp", "chbasic_gpu.cpp", "tipsphil_gpu.cpp", "sips_gpu.cpp", "meso_b200.cpp"]
 
 

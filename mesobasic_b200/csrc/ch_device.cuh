@@ -419,6 +419,10 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
 struct FhCol {
     double T, kT, chi, D;  // TIPSphil / TIPSbathPHIL: temperature, kT, chi, clamped D
     double scale;          // SIPS: mobility scale 0.95 + 0.25*log(1.0225 - chi fraction)
+    // The reciprocal mobility of fh_site_r as a quotient q = f''/Dp:
+    // q > qlo -> rlo and q < qhi -> rhi (the reference's clamps, their
+    // reciprocals formed as the reference forms them), else q * fac.
+    double Dm, invN, conv, qlo, qhi, rlo, rhi, fac;  // conv: Mweight/Mvolume (phi to g/L)
 };
 
 __device__ __forceinline__ FhCol fh_column(const FhDev& F, int x, double cs, double dt)
@@ -438,6 +442,15 @@ __device__ __forceinline__ FhCol fh_column(const FhDev& F, int x, double cs, dou
             k.chi = F.chiPN;
         const double frac = A::div(A::sub(k.chi, F.chiPS), A::sub(F.chiPN, F.chiPS));
         k.scale = A::add(0.95, A::mul(0.25, log(A::sub(1.0225, frac))));
+        // SIPS.cpp:203-206: Mc in [0.00001, 1], then mob = Mc * scale
+        k.Dm = F.D0;
+        k.invN = A::div(1.0, F.N);
+        k.conv = A::div(F.Mweight, F.Mvolume);
+        k.qlo = 100000.0;
+        k.qhi = 1.0;
+        k.rlo = A::div(1.0, A::mul(0.00001, k.scale));
+        k.rhi = A::div(1.0, A::mul(1.0, k.scale));
+        k.fac = A::div(1.0, k.scale);
         return k;
     }
     // temperature of the step: a uniform ramp, or the bath profile along x
@@ -452,6 +465,18 @@ __device__ __forceinline__ FhCol fh_column(const FhDev& F, int x, double cs, dou
     k.chi = A::add(A::div(F.alpha, k.T), F.beta);
     k.D = A::mul(F.D0, A::div(k.T, F.Tinit));
     if (k.D > F.D0) k.D = F.D0;
+    // TIPSphil.cpp:172-175: Mc < 0.000001 -> 0.000001, then Mc > D0 -> D0,
+    // then the crystallisation factor 0.001
+    const bool cryst = k.T <= F.Tcrystal;
+    const double mlo = 0.000001 > F.D0 ? F.D0 : 0.000001;
+    k.Dm = k.D;
+    k.invN = A::div(1.0, F.N);
+    k.conv = A::div(F.Mweight, F.Mvolume);
+    k.qlo = 1000000.0;
+    k.qhi = A::div(1.0, F.D0);
+    k.rlo = A::div(1.0, cryst ? A::mul(mlo, 0.001) : mlo);
+    k.rhi = A::div(1.0, cryst ? A::mul(F.D0, 0.001) : F.D0);
+    k.fac = cryst ? 1000.0 : 1.0;
     return k;
 }
 
@@ -533,6 +558,45 @@ __device__ __forceinline__ void fh_site(const FhDev& F, double cc, double lapc, 
     fh_site_col(F, fh_column(F, x, cs, dt), cc, lapc, kap, mu, mob);
 }
 
+// mu and the reciprocal mobility 1/mob of one site, as the update passes
+// use them.  For TIPSphil, TIPSbathPHIL and SIPS at 0 < cc < 1 (the sites of
+// a field inside the Flory-Huggins range) the mobility is taken as one
+// quotient: with u = 1 - cc the second derivative is
+// f'' = kT (u + N cc) / (2 N cc u), so
+//   1/mob = f'' / Dp = kT (u + N cc) / (2 N cc u Dm e),   e = exp(-gamma phi^nu),
+// and the reference's clamps on Mc become bounds on that quotient, the
+// clamped values' reciprocals formed per column as the reference forms them
+// (FhCol).  That is one division where the reference takes six
+// (1/(N cc), 1/(1 - cc), the conversion to g/L, Dp/f'', 1/Mc, and the
+// 1/N of mu, here a product with 1/N); the result agrees with the
+// reference's to a few ulp.  Everywhere else (cc <= 0, cc >= 1, NaN) and
+// for kFhLinear: fh_site_col's reference-order arithmetic and 1/mob.
+// Explicit fma and rounded operations, so every kernel that inlines this
+// forms the same bits.
+__device__ __forceinline__ void fh_site_r(const FhDev& F, const FhCol& k, double cc, double lapc, double kap,
+                                          double* mu, double* rmob)
+{
+    using A = Arith<double>;
+    if (F.model == kFhLinear || !(cc > 0.0 && cc < 1.0)) {
+        double mob;
+        fh_site_col(F, k, cc, lapc, kap, mu, &mob);
+        *rmob = A::div(1.0, mob);
+        return;
+    }
+    const double u = A::sub(1.0, cc);
+    const double lc = log(cc), lu = log(u);
+    // ((log(cc) + 1)/N - log(1 - cc) - 1 + chi (1 - 2 cc)), times kT for TIPSphil
+    double df = A::add(A::sub(A::sub(A::mul(A::add(lc, 1.0), k.invN), lu), 1.0), A::mul(k.chi, fma(-2.0, cc, 1.0)));
+    if (F.model != kFhSips) df = A::mul(df, k.kT);
+    *mu = fma(-kap, lapc, df);
+    const double phi = A::mul(cc, k.conv);
+    const double e = exp(A::mul(-F.gamma, fh_pow(phi, F.nu)));
+    const double num = A::mul(k.kT, fma(F.N, cc, u));
+    const double den = A::mul(A::mul(A::mul(2.0, A::mul(F.N, cc)), u), A::mul(k.Dm, e));
+    const double q = A::div(num, den);
+    *rmob = q > k.qlo ? k.rlo : (q < k.qhi ? k.rhi : A::mul(q, k.fac));
+}
+
 // One axis of SfieldFD::Laplacian(const SfieldFD& mob) (SfieldFD.cpp:333-355)
 // from the reciprocal mobilities rm, rp, ro of the minus, plus and centre
 // sites: b1 = 2/(1/mob- + 1/mob0), b2 = 2/(1/mob+ + 1/mob0),
@@ -545,6 +609,42 @@ __device__ __forceinline__ double fh_axis_r(double am, double ap, double a0, dou
     const double b2 = A::div(2.0, A::add(rp, ro));
     const double num = A::sub(A::add(A::mul(am, b1), A::mul(ap, b2)), A::mul(A::add(b1, b2), a0));
     return divide ? A::div(num, coef) : A::mul(num, coef);
+}
+
+// One axis of the same divergence as a fraction n/q: with the face sums
+// s1 = 1/mob- + 1/mob0 and s2 = 1/mob+ + 1/mob0 the faces are 2/s1 and
+// 2/s2, and (a- b1 + a+ b2 - (b1 + b2) a0)/d^2 = 2 n/q with
+// n = (a- - a0) s2 + (a+ - a0) s1 and q = s1 s2 d^2 (or n times the
+// multiplier 1/d^2).
+struct FhFrac {
+    double n, q;
+};
+__device__ __forceinline__ FhFrac fh_axis_frac(double am, double ap, double a0, double rm, double rp, double ro,
+                                               double coef, bool divide)
+{
+    using A = Arith<double>;
+    const double s1 = A::add(rm, ro), s2 = A::add(rp, ro);
+    double n = fma(A::sub(am, a0), s2, A::mul(A::sub(ap, a0), s1));
+    double q = A::mul(s1, s2);
+    if (divide) q = A::mul(q, coef);
+    else n = A::mul(n, coef);
+    return {n, q};
+}
+
+// The divergence of a site of a TIPSphil, TIPSbathPHIL or SIPS field from
+// its axes' fractions over one common denominator, one division where the
+// reference's form takes six (nine with unequal spacing):
+// 2 (nx qy qz + ny qx qz + nz qx qy) / (qx qy qz), without y when flat.
+// The face sums are at most twice the largest reciprocal mobility the
+// models' clamps allow (about 2e9), so the products stay far inside the
+// double range.  Agrees with the per-axis form to a few ulp of its terms.
+__device__ __forceinline__ double fh_div_frac(FhFrac x, FhFrac y, FhFrac z, bool flat)
+{
+    using A = Arith<double>;
+    if (flat) return A::div(A::mul(2.0, fma(x.n, z.q, A::mul(z.n, x.q))), A::mul(x.q, z.q));
+    const double qxy = A::mul(x.q, y.q);
+    const double nxy = fma(x.n, y.q, A::mul(y.n, x.q));
+    return A::div(A::mul(2.0, fma(nxy, z.q, A::mul(z.n, qxy))), A::mul(qxy, z.q));
 }
 
 }  // namespace mg

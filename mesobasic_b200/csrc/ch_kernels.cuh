@@ -622,6 +622,17 @@ __global__ void ch_noise_kernel(JobDev* job)
 //    the constant Mpp (Mnn): the fields step independently.  The GPU takes
 //    the same arithmetic.
 
+// The scalars of a job the variable-mobility passes use at every site,
+// copied out of JobDev once per thread.
+struct FhView {
+    int nx, ny, nz, flags;
+    double cx, cy, cz, kap, dt, noise, cutoff;
+};
+__device__ __forceinline__ FhView fh_view(const JobDev& J)
+{
+    return {J.nx, J.ny, J.nz, J.flags, J.cx, J.cy, J.cz, J.kap, J.dtM_dt, J.noise, J.noise_cutoff};
+}
+
 // The neighbours of site s one step down / up an axis of length n and
 // stride st, from its coordinate i: the periodic wrap, or on a no-flux axis
 // the site itself (the ghost copy): the site at coordinate
@@ -639,22 +650,26 @@ __device__ __forceinline__ size_t fh_up(size_t s, int i, int n, size_t st, size_
 // Pass 1: mu and the reciprocal mobility 1/mob of every site (F.mu, F.mob).
 // A thread keeps one x for all its sites (the grid's stride is a multiple
 // of nx), so the per-x constants of the step (fh_column) are formed once.
-__global__ void fh_mu_mob_kernel(JobDev* job)
+__global__ void __launch_bounds__(256, 4) fh_mu_mob_kernel(JobDev* job)
 {
     using A = Arith<double>;
     const JobDev& J = *job;
     const FhDev& F = *J.fh;
+    // the job's scalars, read once (the field stores below may alias *job
+    // as far as the compiler knows); the model's fields stay in memory,
+    // which measured faster here than a copy that spills
+    const FhView V = fh_view(J);
     const int nx = J.nx, ny = J.ny, nz = J.nz;
     const size_t n = (size_t)nx * ny * nz;
     if (J.step >= J.target) return;
     const double* __restrict__ c = static_cast<const double*>(J.buf[J.step & 1]);
     // the step being taken (PFApp passes it as current_step)
     const double cs = (double)(J.step + 1);
-    const bool pX = J.flags & JF_PER_X, pY = J.flags & JF_PER_Y, pZ = J.flags & JF_PER_Z;
+    const bool pX = V.flags & JF_PER_X, pY = V.flags & JF_PER_Y, pZ = V.flags & JF_PER_Z;
     const size_t first = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const size_t stride = (size_t)gridDim.x * blockDim.x;  // a multiple of nx (the host's launch)
     const int x = (int)(first % nx);
-    const FhCol col = fh_column(F, x, cs, J.dtM_dt);
+    const FhCol col = fh_column(F, x, cs, V.dt);
     // the row (y, z) of site s, advanced by the stride's whole rows without
     // a division per site
     const size_t r0 = first / nx, dr = stride / nx;
@@ -668,17 +683,17 @@ __global__ void fh_mu_mob_kernel(JobDev* job)
         const double xp = c[fh_up(s, x, nx, 1, wx, pX)], xm = c[fh_down(s, x, 1, wx, pX)];
         const double zp = c[fh_up(s, z, nz, sz, wz, pZ)], zm = c[fh_down(s, z, sz, wz, pZ)];
         double lapc;
-        if (J.flags & JF_FLAT) {
-            lapc = A::add(axis_term(xp, xm, cc, J.cx, J.flags & JF_DIV_X), axis_term(zp, zm, cc, J.cz, J.flags & JF_DIV_Z));
+        if (V.flags & JF_FLAT) {
+            lapc = A::add(axis_term(xp, xm, cc, V.cx, V.flags & JF_DIV_X), axis_term(zp, zm, cc, V.cz, V.flags & JF_DIV_Z));
         } else {
             const double yp = c[fh_up(s, y, ny, sy, wy, pY)], ym = c[fh_down(s, y, sy, wy, pY)];
-            lapc = A::add(A::add(axis_term(xp, xm, cc, J.cx, J.flags & JF_DIV_X), axis_term(yp, ym, cc, J.cy, J.flags & JF_DIV_Y)),
-                          axis_term(zp, zm, cc, J.cz, J.flags & JF_DIV_Z));
+            lapc = A::add(A::add(axis_term(xp, xm, cc, V.cx, V.flags & JF_DIV_X), axis_term(yp, ym, cc, V.cy, V.flags & JF_DIV_Y)),
+                          axis_term(zp, zm, cc, V.cz, V.flags & JF_DIV_Z));
         }
-        double mu, mob;
-        fh_site_col(F, col, cc, lapc, J.kap, &mu, &mob);
+        double mu, rmob;
+        fh_site_r(F, col, cc, lapc, V.kap, &mu, &rmob);
         F.mu[s] = mu;
-        F.mob[s] = A::div(1.0, mob);  // the reciprocal every face of the site uses
+        F.mob[s] = rmob;  // the reciprocal every face of the site uses
         y += dy;
         z += dz;
         if (y >= ny) {
@@ -691,13 +706,16 @@ __global__ void fh_mu_mob_kernel(JobDev* job)
 // Pass 2: c += dt * div(mob grad mu) (SfieldFD::Laplacian(const SfieldFD&),
 // SfieldFD.cpp:333-355) from mu and the reciprocal mobilities of pass 1:
 // each face's harmonic mean 2/(1/mob_a + 1/mob_b) from the two stored
-// reciprocals -- the reference's operands in its order, so the same value.
+// reciprocals.  A constant-mobility field (SIPSternary) takes the
+// reference's per-axis form with its operands in its order, so the same
+// value; the Flory-Huggins models take the three axes over one common
+// denominator (fh_div_frac), one division per site instead of six.
 // Then the per-step noise (TIPSphil.cpp:200-209), as ch_noise_kernel adds
 // it: a thread takes four consecutive sites, one draw of the counter-based
 // generator (site/4, step).
-__device__ __forceinline__ double fh_update_site(const JobDev& J, const double* __restrict__ c,
+__device__ __forceinline__ double fh_update_site(const FhView& J, const double* __restrict__ c,
                                                  const double* __restrict__ mu, const double* __restrict__ rmob,
-                                                 size_t s, int x, int y, int z)
+                                                 size_t s, int x, int y, int z, bool linear)
 {
     using A = Arith<double>;
     const int nx = J.nx, ny = J.ny, nz = J.nz;
@@ -707,58 +725,93 @@ __device__ __forceinline__ double fh_update_site(const JobDev& J, const double* 
     const size_t wx = (size_t)(nx - 1), wy = (size_t)(ny - 1) * sy, wz = (size_t)(nz - 1) * sz;
     const size_t ixm = fh_down(s, x, 1, wx, pX), ixp = fh_up(s, x, nx, 1, wx, pX);
     const size_t izm = fh_down(s, z, sz, wz, pZ), izp = fh_up(s, z, nz, sz, wz, pZ);
-    const double lx = fh_axis_r(mu[ixm], mu[ixp], a0, rmob[ixm], rmob[ixp], ro, J.cx, J.flags & JF_DIV_X);
-    const double lz = fh_axis_r(mu[izm], mu[izp], a0, rmob[izm], rmob[izp], ro, J.cz, J.flags & JF_DIV_Z);
+    const bool flat = J.flags & JF_FLAT;
+    size_t iym = s, iyp = s;
+    if (!flat) iym = fh_down(s, y, sy, wy, pY), iyp = fh_up(s, y, ny, sy, wy, pY);
     double lap;
-    if (J.flags & JF_FLAT) {
-        lap = A::add(lx, lz);
+    if (linear) {
+        // constant mobility (SIPSternary): the reference's per-axis form, bit for bit
+        const double lx = fh_axis_r(mu[ixm], mu[ixp], a0, rmob[ixm], rmob[ixp], ro, J.cx, J.flags & JF_DIV_X);
+        const double lz = fh_axis_r(mu[izm], mu[izp], a0, rmob[izm], rmob[izp], ro, J.cz, J.flags & JF_DIV_Z);
+        if (flat) {
+            lap = A::add(lx, lz);
+        } else {
+            const double ly = fh_axis_r(mu[iym], mu[iyp], a0, rmob[iym], rmob[iyp], ro, J.cy, J.flags & JF_DIV_Y);
+            lap = A::add(A::add(lx, ly), lz);
+        }
     } else {
-        const size_t iym = fh_down(s, y, sy, wy, pY), iyp = fh_up(s, y, ny, sy, wy, pY);
-        const double ly = fh_axis_r(mu[iym], mu[iyp], a0, rmob[iym], rmob[iyp], ro, J.cy, J.flags & JF_DIV_Y);
-        lap = A::add(A::add(lx, ly), lz);
+        const FhFrac fx = fh_axis_frac(mu[ixm], mu[ixp], a0, rmob[ixm], rmob[ixp], ro, J.cx, J.flags & JF_DIV_X);
+        const FhFrac fz = fh_axis_frac(mu[izm], mu[izp], a0, rmob[izm], rmob[izp], ro, J.cz, J.flags & JF_DIV_Z);
+        FhFrac fy{0.0, 1.0};
+        if (!flat) fy = fh_axis_frac(mu[iym], mu[iyp], a0, rmob[iym], rmob[iyp], ro, J.cy, J.flags & JF_DIV_Y);
+        lap = fh_div_frac(fx, fy, fz, flat);
     }
-    return A::add(c[s], A::mul(J.dtM_dt, lap));  // c += dt * lap (TIPSphil.cpp:194)
+    return A::add(c[s], A::mul(J.dt, lap));  // c += dt * lap (TIPSphil.cpp:194)
 }
 
-__global__ void fh_update_kernel(JobDev* job)
+// A warp takes 128 consecutive sites, lane l the sites base + 32e + l
+// (e = 0..3), so every gather of mu and 1/mob is one coalesced run per warp.
+// The noise counter keeps its grouping (site/4, step): lane l draws the
+// words of group base/4 + l, and the lane of a site takes its word from the
+// group's lane by shuffles, the same word the site gets in ch_noise_kernel.
+__global__ void __launch_bounds__(256, 4) fh_update_kernel(JobDev* job)
 {
     using A = Arith<double>;
     const JobDev& J = *job;
-    const FhDev& F = *J.fh;
+    // the model's and the job's fields, read once: as far as the compiler
+    // knows the field stores below may alias them, so it would read them
+    // again for every site
+    const FhDev F = *J.fh;
+    const FhView V = fh_view(J);
     const long long n = (long long)J.nx * J.ny * J.nz;
-    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // sites 4g .. 4g+3
-    if (J.step >= J.target || 4 * g >= n) return;
+    const int lane = threadIdx.x & 31;
+    const long long base = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 128;  // the warp's sites
+    if (J.step >= J.target || base >= n) return;  // uniform over the warp
     const int par = (int)(J.step & 1);
     const double* __restrict__ c = static_cast<const double*>(J.buf[par]);
     double* __restrict__ out = static_cast<double*>(J.buf[par ^ 1]);
+    const bool linear = F.model == kFhLinear;
     uint32_t word[4] = {0u, 0u, 0u, 0u};
     const bool noisy = J.noise != 0.0;
     if (noisy) {
         const long long st = J.step + 1;  // the step being taken
+        const long long g = base / 4 + lane;  // sites 4g .. 4g+3
         const uint2 key = make_uint2((uint32_t)J.noise_seed, (uint32_t)(J.noise_seed >> 32));
         const uint4 w = philox4x32_10(make_uint4((uint32_t)g, (uint32_t)(g >> 32), (uint32_t)st, (uint32_t)(st >> 32)), key);
         word[0] = w.x, word[1] = w.y, word[2] = w.z, word[3] = w.w;
     }
-    // coordinates of the first site; the others follow along x
-    const long long s0 = 4 * g, r0 = s0 / J.nx;
-    int x = (int)(s0 - r0 * J.nx), y = (int)(r0 % J.ny), z = (int)(r0 / J.ny);
+    // coordinates of the lane's first site; each next one lies 32 sites on
+    long long s = base + lane;
+    const long long r0 = s / J.nx;
+    int x = (int)(s - r0 * J.nx), y = (int)(r0 % J.ny), z = (int)(r0 / J.ny);
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-        const long long s = s0 + e;
-        if (s >= n) break;
-        if (e > 0 && ++x == J.nx) {
-            x = 0;
-            if (++y == J.ny) {
-                y = 0;
-                ++z;
+        if (e > 0) {
+            s += 32;
+            x += 32;
+            while (x >= V.nx) {
+                x -= V.nx;
+                if (++y == V.ny) {
+                    y = 0;
+                    ++z;
+                }
             }
         }
-        double v = fh_update_site(J, c, F.mu, F.mob, (size_t)s, x, y, z);
+        // the word of site s: group s/4 is lane 8e + l/4's, component s & 3 = l & 3
+        uint32_t wd = 0u;
+        if (noisy) {
+            const int src = 8 * e + (lane >> 2), k = lane & 3;
+            const uint32_t w0 = __shfl_sync(0xffffffffu, word[0], src), w1 = __shfl_sync(0xffffffffu, word[1], src);
+            const uint32_t w2 = __shfl_sync(0xffffffffu, word[2], src), w3 = __shfl_sync(0xffffffffu, word[3], src);
+            wd = k == 0 ? w0 : (k == 1 ? w1 : (k == 2 ? w2 : w3));
+        }
+        if (s >= n) continue;
+        double v = fh_update_site(V, c, F.mu, F.mob, (size_t)s, x, y, z, linear);
         if (noisy) {
             // SIPS.cpp:239-240: no noise at or above the cutoff (+inf elsewhere)
-            const double r = A::add(A::mul((double)word[e], 2.3283064365386963e-10), 1.1641532182693481e-10);
-            const double val = v >= J.noise_cutoff ? 0.0 : A::mul(J.noise, A::sub(r, 0.5));
-            v = A::add(v, A::mul(J.dtM_dt, val));
+            const double r = A::add(A::mul((double)wd, 2.3283064365386963e-10), 1.1641532182693481e-10);
+            const double val = v >= V.cutoff ? 0.0 : A::mul(V.noise, A::sub(r, 0.5));
+            v = A::add(v, A::mul(V.dt, val));
         }
         out[s] = v;
     }

@@ -147,6 +147,7 @@ __global__ void __launch_bounds__(kFhBlock, 1) fh_march_kernel(StepArgs a)
         double* g = dst + (long long)zfirst * pstride + site_row;
         const long long gstep = (long long)dir * pstride;
         const bool noisy = J->noise != 0.0;
+        const bool linear = F.model == kFhLinear;
         const double noise = J->noise, cutoff = J->noise_cutoff;
         const uint2 key = make_uint2((uint32_t)J->noise_seed, (uint32_t)(J->noise_seed >> 32));
         const long long st = step + 1;  // the noise counter's step (the step just taken)
@@ -228,9 +229,7 @@ __global__ void __launch_bounds__(kFhBlock, 1) fh_march_kernel(StepArgs a)
                         const double ym = FLAT ? c0 : up[e], yp = FLAT ? c0 : dn[e];
                         const double lapc =
                             lap7<double, FLAT, false>(c0, xp, xm, yp, ym, cn[e], cp[e], cx, cy, cz, divX, divY, divZ);
-                        double mob;
-                        fh_site_col(F, coltab[x0 + e], c0, lapc, kap, &mu[e], &mob);
-                        rm[e] = A::div(1.0, mob);
+                        fh_site_r(F, coltab[x0 + e], c0, lapc, kap, &mu[e], &rm[e]);
                     }
                     sts4d(mubase + msl * mplaneB + mOwn, mu);
                     sts4d(rmbase + msl * mplaneB + mOwn, rm);
@@ -271,18 +270,24 @@ __global__ void __launch_bounds__(kFhBlock, 1) fh_march_kernel(StepArgs a)
                     for (int e = 0; e < 4; ++e) {
                         const double am = e > 0 ? a0[e - 1] : axm0, rmm = e > 0 ? r0[e - 1] : rxm0;
                         const double ap = e < 3 ? a0[e + 1] : axp3, rpp = e < 3 ? r0[e + 1] : rxp3;
-                        const double lx = fh_axis_r(am, ap, a0[e], rmm, rpp, r0[e], cx, divX);
                         const double zm = sLo ? a0[e] : az_m[e], rzm = sLo ? r0[e] : rz_m[e];
                         const double zp = sHi ? a0[e] : az_p[e], rzp = sHi ? r0[e] : rz_p[e];
-                        const double lz = fh_axis_r(zm, zp, a0[e], rzm, rzp, r0[e], cz, divZ);
+                        double ym = a0[e], rym = r0[e], yp = a0[e], ryp = r0[e];
+                        if (!FLAT) {
+                            ym = subUp ? a0[e] : ay_m[e], rym = subUp ? r0[e] : ry_m[e];
+                            yp = subDn ? a0[e] : ay_p[e], ryp = subDn ? r0[e] : ry_p[e];
+                        }
                         double lap;
-                        if (FLAT) {
-                            lap = A::add(lx, lz);
+                        if (linear) {
+                            const double lx = fh_axis_r(am, ap, a0[e], rmm, rpp, r0[e], cx, divX);
+                            const double lz = fh_axis_r(zm, zp, a0[e], rzm, rzp, r0[e], cz, divZ);
+                            lap = FLAT ? A::add(lx, lz)
+                                       : A::add(A::add(lx, fh_axis_r(ym, yp, a0[e], rym, ryp, r0[e], cy, divY)), lz);
                         } else {
-                            const double ym = subUp ? a0[e] : ay_m[e], rym = subUp ? r0[e] : ry_m[e];
-                            const double yp = subDn ? a0[e] : ay_p[e], ryp = subDn ? r0[e] : ry_p[e];
-                            const double ly = fh_axis_r(ym, yp, a0[e], rym, ryp, r0[e], cy, divY);
-                            lap = A::add(A::add(lx, ly), lz);
+                            const FhFrac fx = fh_axis_frac(am, ap, a0[e], rmm, rpp, r0[e], cx, divX);
+                            const FhFrac fz = fh_axis_frac(zm, zp, a0[e], rzm, rzp, r0[e], cz, divZ);
+                            const FhFrac fy = FLAT ? FhFrac{0.0, 1.0} : fh_axis_frac(ym, yp, a0[e], rym, ryp, r0[e], cy, divY);
+                            lap = fh_div_frac(fx, fy, fz, FLAT);
                         }
                         double v = A::add(cp[e], A::mul(dt, lap));  // c += dt * lap (TIPSphil.cpp:194)
                         if (noisy) {
