@@ -638,11 +638,15 @@ __device__ __forceinline__ FhView fh_view(const JobDev& J)
 // the site itself (the ghost copy): the site at coordinate
 // wrap_or_clamp(i -/+ 1, n) on that axis, without its modulo and without
 // forming the index from (x, y, z).
-__device__ __forceinline__ size_t fh_down(size_t s, int i, size_t st, size_t span, bool per)
+// I is the index type: 32-bit for fields of fewer than 2^31 sites (one
+// integer instruction per step where 64-bit indices take two), else size_t.
+template <typename I>
+__device__ __forceinline__ I fh_down(I s, int i, I st, I span, bool per)
 {
     return i > 0 ? s - st : (per ? s + span : s);
 }
-__device__ __forceinline__ size_t fh_up(size_t s, int i, int n, size_t st, size_t span, bool per)
+template <typename I>
+__device__ __forceinline__ I fh_up(I s, int i, int n, I st, I span, bool per)
 {
     return i < n - 1 ? s + st : (per ? s - span : s);
 }
@@ -650,37 +654,31 @@ __device__ __forceinline__ size_t fh_up(size_t s, int i, int n, size_t st, size_
 // Pass 1: mu and the reciprocal mobility 1/mob of every site (F.mu, F.mob).
 // A thread keeps one x for all its sites (the grid's stride is a multiple
 // of nx), so the per-x constants of the step (fh_column) are formed once.
-__global__ void __launch_bounds__(256, 4) fh_mu_mob_kernel(JobDev* job)
+template <typename I>
+__device__ __forceinline__ void fh_mu_mob_sites(const JobDev& J, const FhDev& F, const FhView& V)
 {
     using A = Arith<double>;
-    const JobDev& J = *job;
-    const FhDev& F = *J.fh;
-    // the job's scalars, read once (the field stores below may alias *job
-    // as far as the compiler knows); the model's fields stay in memory,
-    // which measured faster here than a copy that spills
-    const FhView V = fh_view(J);
-    const int nx = J.nx, ny = J.ny, nz = J.nz;
-    const size_t n = (size_t)nx * ny * nz;
-    if (J.step >= J.target) return;
+    const int nx = V.nx, ny = V.ny, nz = V.nz;
+    const I n = (I)nx * ny * nz;
     const double* __restrict__ c = static_cast<const double*>(J.buf[J.step & 1]);
     // the step being taken (PFApp passes it as current_step)
     const double cs = (double)(J.step + 1);
     const bool pX = V.flags & JF_PER_X, pY = V.flags & JF_PER_Y, pZ = V.flags & JF_PER_Z;
-    const size_t first = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t stride = (size_t)gridDim.x * blockDim.x;  // a multiple of nx (the host's launch)
+    const I first = (I)blockIdx.x * blockDim.x + threadIdx.x;
+    const I stride = (I)gridDim.x * blockDim.x;  // a multiple of nx (the host's launch)
     const int x = (int)(first % nx);
     const FhCol col = fh_column(F, x, cs, V.dt);
     // the row (y, z) of site s, advanced by the stride's whole rows without
     // a division per site
-    const size_t r0 = first / nx, dr = stride / nx;
+    const I r0 = first / nx, dr = stride / nx;
     int y = (int)(r0 % ny), z = (int)(r0 / ny);
     const int dy = (int)(dr % ny), dz = (int)(dr / ny);
     // strides and wrap spans of the three axes
-    const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
-    const size_t wx = (size_t)(nx - 1), wy = (size_t)(ny - 1) * sy, wz = (size_t)(nz - 1) * sz;
-    for (size_t s = first; s < n; s += stride) {
+    const I sy = (I)nx, sz = (I)nx * ny;
+    const I wx = (I)(nx - 1), wy = (I)(ny - 1) * sy, wz = (I)(nz - 1) * sz;
+    for (I s = first; s < n; s += stride) {
         const double cc = c[s];
-        const double xp = c[fh_up(s, x, nx, 1, wx, pX)], xm = c[fh_down(s, x, 1, wx, pX)];
+        const double xp = c[fh_up(s, x, nx, (I)1, wx, pX)], xm = c[fh_down(s, x, (I)1, wx, pX)];
         const double zp = c[fh_up(s, z, nz, sz, wz, pZ)], zm = c[fh_down(s, z, sz, wz, pZ)];
         double lapc;
         if (V.flags & JF_FLAT) {
@@ -703,6 +701,18 @@ __global__ void __launch_bounds__(256, 4) fh_mu_mob_kernel(JobDev* job)
     }
 }
 
+__global__ void __launch_bounds__(256, 4) fh_mu_mob_kernel(JobDev* job)
+{
+    const JobDev& J = *job;
+    if (J.step >= J.target) return;
+    // the job's scalars, read once (the field stores may alias *job as far
+    // as the compiler knows); the model's fields stay in memory, which
+    // measured faster here than a copy that spills
+    const FhView V = fh_view(J);
+    if ((long long)V.nx * V.ny * V.nz < (1LL << 31)) fh_mu_mob_sites<uint32_t>(J, *J.fh, V);
+    else fh_mu_mob_sites<size_t>(J, *J.fh, V);
+}
+
 // Pass 2: c += dt * div(mob grad mu) (SfieldFD::Laplacian(const SfieldFD&),
 // SfieldFD.cpp:333-355) from mu and the reciprocal mobilities of pass 1:
 // each face's harmonic mean 2/(1/mob_a + 1/mob_b) from the two stored
@@ -713,20 +723,21 @@ __global__ void __launch_bounds__(256, 4) fh_mu_mob_kernel(JobDev* job)
 // Then the per-step noise (TIPSphil.cpp:200-209), as ch_noise_kernel adds
 // it: a thread takes four consecutive sites, one draw of the counter-based
 // generator (site/4, step).
+template <typename I>
 __device__ __forceinline__ double fh_update_site(const FhView& J, const double* __restrict__ c,
                                                  const double* __restrict__ mu, const double* __restrict__ rmob,
-                                                 size_t s, int x, int y, int z, bool linear)
+                                                 I s, int x, int y, int z, bool linear)
 {
     using A = Arith<double>;
     const int nx = J.nx, ny = J.ny, nz = J.nz;
     const bool pX = J.flags & JF_PER_X, pY = J.flags & JF_PER_Y, pZ = J.flags & JF_PER_Z;
     const double a0 = mu[s], ro = rmob[s];
-    const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
-    const size_t wx = (size_t)(nx - 1), wy = (size_t)(ny - 1) * sy, wz = (size_t)(nz - 1) * sz;
-    const size_t ixm = fh_down(s, x, 1, wx, pX), ixp = fh_up(s, x, nx, 1, wx, pX);
-    const size_t izm = fh_down(s, z, sz, wz, pZ), izp = fh_up(s, z, nz, sz, wz, pZ);
+    const I sy = (I)nx, sz = (I)nx * ny;
+    const I wx = (I)(nx - 1), wy = (I)(ny - 1) * sy, wz = (I)(nz - 1) * sz;
+    const I ixm = fh_down(s, x, (I)1, wx, pX), ixp = fh_up(s, x, nx, (I)1, wx, pX);
+    const I izm = fh_down(s, z, sz, wz, pZ), izp = fh_up(s, z, nz, sz, wz, pZ);
     const bool flat = J.flags & JF_FLAT;
-    size_t iym = s, iyp = s;
+    I iym = s, iyp = s;
     if (!flat) iym = fh_down(s, y, sy, wy, pY), iyp = fh_up(s, y, ny, sy, wy, pY);
     double lap;
     if (linear) {
@@ -771,6 +782,7 @@ __global__ void __launch_bounds__(256, 4) fh_update_kernel(JobDev* job)
     const double* __restrict__ c = static_cast<const double*>(J.buf[par]);
     double* __restrict__ out = static_cast<double*>(J.buf[par ^ 1]);
     const bool linear = F.model == kFhLinear;
+    const bool small = n < (1LL << 31);  // 32-bit site indices
     uint32_t word[4] = {0u, 0u, 0u, 0u};
     const bool noisy = J.noise != 0.0;
     if (noisy) {
@@ -806,7 +818,8 @@ __global__ void __launch_bounds__(256, 4) fh_update_kernel(JobDev* job)
             wd = k == 0 ? w0 : (k == 1 ? w1 : (k == 2 ? w2 : w3));
         }
         if (s >= n) continue;
-        double v = fh_update_site(V, c, F.mu, F.mob, (size_t)s, x, y, z, linear);
+        double v = small ? fh_update_site(V, c, F.mu, F.mob, (uint32_t)s, x, y, z, linear)
+                         : fh_update_site(V, c, F.mu, F.mob, (size_t)s, x, y, z, linear);
         if (noisy) {
             // SIPS.cpp:239-240: no noise at or above the cutoff (+inf elsewhere)
             const double r = A::add(A::mul((double)wd, 2.3283064365386963e-10), 1.1641532182693481e-10);
