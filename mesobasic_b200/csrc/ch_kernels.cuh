@@ -720,9 +720,9 @@ __global__ void __launch_bounds__(256, 4) fh_mu_mob_kernel(JobDev* job)
 // reference's per-axis form with its operands in its order, so the same
 // value; the Flory-Huggins models take the three axes over one common
 // denominator (fh_div_frac), one division per site instead of six.
-// Then the per-step noise (TIPSphil.cpp:200-209), as ch_noise_kernel adds
-// it: a thread takes four consecutive sites, one draw of the counter-based
-// generator (site/4, step).
+// Then the per-step noise (TIPSphil.cpp:200-209) with the word
+// ch_noise_kernel gives the site: one draw of the counter-based generator
+// per four consecutive sites (site/4, step).
 template <typename I>
 __device__ __forceinline__ double fh_update_site(const FhView& J, const double* __restrict__ c,
                                                  const double* __restrict__ mu, const double* __restrict__ rmob,
